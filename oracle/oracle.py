@@ -1,0 +1,246 @@
+"""TEST INFRASTRUCTURE (the oracle), not product code.
+
+ctypes binding of oracle/liboracle.so (the project's CPU restatement of the
+reference backprojection, oracle/bp_oracle.c) and of oracle/_ref/libref_bp*.so
+(the reference's own run_bp compiled from its sources by oracle/Makefile).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module, and only as the checker.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = {}
+
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_c = ctypes
+
+
+def build() -> None:
+    """Compile liboracle.so, and the reference harness when the reference
+    sources are present (make is a no-op when everything is up to date)."""
+    import subprocess
+
+    targets = ["all"] if os.path.isdir("/root/reference/src") else [os.path.join(HERE, "liboracle.so")]
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        L.oracle_range_compress_fp64.argtypes = [_c.c_int, _c.c_int, _c.c_int, _f32p, _c.c_void_p, _f64p]
+        L.oracle_range_compress_ref32.argtypes = [_c.c_int, _c.c_int, _f32p, _f32p]
+        bp_geo = [_f64p] * 5 + [_c.c_double] + [_c.c_int] * 3 + [_c.c_double] * 6
+        L.oracle_bp_fp64.argtypes = [_c.c_int, _c.c_int, _f64p] + bp_geo + [_f64p]
+        L.oracle_bp_fp64_pixels.argtypes = [_c.c_int, _c.c_int, _f64p] + bp_geo + [_c.c_longlong, _i64p, _f64p]
+        L.oracle_bp_ref32.argtypes = ([_c.c_int, _c.c_int, _f32p] + [_f32p] * 5 + [_c.c_float, _c.c_int, _c.c_int]
+                                      + [_c.c_float] * 4 + [_f32p])
+        L.oracle_range_compress_ref64.argtypes = [_c.c_int, _c.c_int, _f64p, _f64p]
+        L.oracle_bp_ref64.argtypes = ([_c.c_int, _c.c_int, _f64p] + [_f64p] * 5 + [_c.c_double, _c.c_int, _c.c_int]
+                                      + [_c.c_double] * 4 + [_f64p])
+        L.oracle_dft_c128.argtypes = [_c.c_int, _f64p, _f64p, _c.c_int]
+        for f in ("oracle_range_compress_fp64", "oracle_range_compress_ref32", "oracle_bp_fp64",
+                  "oracle_bp_fp64_pixels", "oracle_bp_ref32", "oracle_dft_c128", "oracle_range_compress_ref64",
+                  "oracle_bp_ref64"):
+            getattr(L, f).restype = _c.c_int
+        _LIB = L
+    return _LIB
+
+
+def ref_available(fast: bool = False) -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_bp_fast.so" if fast else "libref_bp.so"))
+
+
+def ref_lib(fast: bool = False):
+    key = "fast" if fast else "strict"
+    if key not in _REF:
+        path = os.path.join(HERE, "_ref", "libref_bp_fast.so" if fast else "libref_bp.so")
+        L = ctypes.CDLL(path)
+        L.ref_focus_bp_f32.argtypes = ([_c.c_int, _c.c_int] + [_f32p] * 6 + [_c.c_int, _c.c_int]
+                                       + [_c.c_float] * 4 + [_f32p, _f32p, _f32p])
+        L.ref_focus_bp_f64.argtypes = ([_c.c_int, _c.c_int] + [_f64p] * 6 + [_c.c_int, _c.c_int]
+                                       + [_c.c_double] * 4 + [_f64p, _f64p, _f64p])
+        L.ref_focus_bp_f32.restype = _c.c_int
+        L.ref_focus_bp_f64.restype = _c.c_int
+        _REF[key] = L
+    return _REF[key]
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise RuntimeError(f"{what} failed with status {rc}")
+
+
+def hamming(K: int) -> np.ndarray:
+    """0.54 - 0.46 cos(2 pi k / (K-1)) (the taper of matlab/formImage3DSAR.m:115-116)."""
+    k = np.arange(K, dtype=np.float64)
+    return 0.54 - 0.46 * np.cos(2.0 * np.pi * k / (K - 1))
+
+
+def window_for(name: Optional[str], K: int) -> Optional[np.ndarray]:
+    if name in (None, "none"):
+        return None
+    if name == "hamming":
+        return hamming(K)
+    raise ValueError(name)
+
+
+def dft(x: np.ndarray, sign: int) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    out = np.empty_like(x)
+    _check(lib().oracle_dft_c128(x.shape[0], x.view(np.float64), out.view(np.float64), sign), "dft")
+    return out
+
+
+def range_compress_fp64(ph: np.ndarray, nfft: int, window: Optional[np.ndarray] = None) -> np.ndarray:
+    ph = np.ascontiguousarray(ph, dtype=np.complex64)
+    Np, K = ph.shape
+    out = np.empty((Np, nfft), dtype=np.complex128)
+    wptr = None
+    if window is not None:
+        window = np.ascontiguousarray(window, dtype=np.float64)
+        wptr = window.ctypes.data
+    _check(lib().oracle_range_compress_fp64(K, Np, nfft, ph.view(np.float32).reshape(-1), wptr,
+                                            out.view(np.float64).reshape(-1)), "range_compress_fp64")
+    return out
+
+
+def _geo(ax, ay, az, r0, f0):
+    return [np.ascontiguousarray(v, dtype=np.float64) for v in (ax, ay, az, r0, f0)]
+
+
+def bp_fp64(rc: np.ndarray, ax, ay, az, r0, f0, max_wr: float, grid) -> np.ndarray:
+    rc = np.ascontiguousarray(rc, dtype=np.complex128)
+    Np, nfft = rc.shape
+    out = np.empty((grid.nz, grid.nx, grid.ny), dtype=np.complex128)
+    _check(lib().oracle_bp_fp64(Np, nfft, rc.view(np.float64).reshape(-1), *_geo(ax, ay, az, r0, f0),
+                                float(max_wr), grid.nx, grid.ny, grid.nz, grid.x0, grid.y0, grid.z0, grid.wx,
+                                grid.wy, grid.wz, out.view(np.float64).reshape(-1)), "bp_fp64")
+    return out
+
+
+def bp_fp64_pixels(rc: np.ndarray, ax, ay, az, r0, f0, max_wr: float, grid, pix: np.ndarray) -> np.ndarray:
+    rc = np.ascontiguousarray(rc, dtype=np.complex128)
+    Np, nfft = rc.shape
+    pix = np.ascontiguousarray(pix, dtype=np.int64)
+    out = np.empty(pix.shape[0], dtype=np.complex128)
+    _check(lib().oracle_bp_fp64_pixels(Np, nfft, rc.view(np.float64).reshape(-1), *_geo(ax, ay, az, r0, f0),
+                                       float(max_wr), grid.nx, grid.ny, grid.nz, grid.x0, grid.y0, grid.z0,
+                                       grid.wx, grid.wy, grid.wz, pix.shape[0], pix,
+                                       out.view(np.float64).reshape(-1)), "bp_fp64_pixels")
+    return out
+
+
+def focus_fp64(scene, pixels: Optional[np.ndarray] = None) -> np.ndarray:
+    """FP64 oracle image of a scenes.Scene (window, zero pad to Nfft, IFFT,
+    fftshift, then BP).  With pixels, only those flat indices are formed."""
+    w = window_for(scene.window, scene.num_range_samples)
+    rc = range_compress_fp64(scene.phase_history, scene.nfft, w)
+    args = (rc, scene.ant_x, scene.ant_y, scene.ant_z, scene.slant_range, scene.start_freq, scene.max_wr,
+            scene.grid)
+    if pixels is None:
+        return bp_fp64(*args)
+    return bp_fp64_pixels(*args, pixels)
+
+
+def pad_for_reference(scene, dtype=np.float32):
+    """The reference has no zero pad or window (cpuBackProjection.hpp:107-110):
+    feed it w.*ph zero-padded from K to Nfft and freq extended at the same step."""
+    K = scene.num_range_samples
+    w = window_for(scene.window, K)
+    ph = scene.phase_history.astype(np.complex128)
+    if w is not None:
+        ph = ph * w[None, :]
+    padded = np.zeros((scene.num_pulses, scene.nfft), dtype=np.complex128)
+    padded[:, :K] = ph
+    freq = scene.start_freq[0] + np.arange(scene.nfft, dtype=np.float64) * scene.delta_freq
+    ctype = np.complex64 if dtype == np.float32 else np.complex128
+    return padded.astype(ctype), freq.astype(dtype)
+
+
+def range_compress_ref32(ph_padded: np.ndarray) -> np.ndarray:
+    ph_padded = np.ascontiguousarray(ph_padded, dtype=np.complex64)
+    Np, nfft = ph_padded.shape
+    out = np.empty_like(ph_padded)
+    _check(lib().oracle_range_compress_ref32(nfft, Np, ph_padded.view(np.float32).reshape(-1),
+                                             out.view(np.float32).reshape(-1)), "range_compress_ref32")
+    return out
+
+
+def bp_ref32(rc: np.ndarray, ax, ay, az, r0, f0, max_wr: float, nx: int, ny: int, x0: float, y0: float,
+             wx: float, wy: float) -> np.ndarray:
+    rc = np.ascontiguousarray(rc, dtype=np.complex64)
+    Np, nfft = rc.shape
+    out = np.empty((nx, ny), dtype=np.complex64)
+    geo = [np.ascontiguousarray(v, dtype=np.float32) for v in (ax, ay, az, r0, f0)]
+    _check(lib().oracle_bp_ref32(Np, nfft, rc.view(np.float32).reshape(-1), *geo, np.float32(max_wr), nx, ny,
+                                 np.float32(x0), np.float32(y0), np.float32(wx), np.float32(wy),
+                                 out.view(np.float32).reshape(-1)), "bp_ref32")
+    return out
+
+
+def range_compress_ref64(ph_padded: np.ndarray) -> np.ndarray:
+    ph_padded = np.ascontiguousarray(ph_padded, dtype=np.complex128)
+    Np, nfft = ph_padded.shape
+    out = np.empty_like(ph_padded)
+    _check(lib().oracle_range_compress_ref64(nfft, Np, ph_padded.view(np.float64).reshape(-1),
+                                             out.view(np.float64).reshape(-1)), "range_compress_ref64")
+    return out
+
+
+def bp_ref64(rc: np.ndarray, ax, ay, az, r0, f0, max_wr: float, nx: int, ny: int, x0: float, y0: float,
+             wx: float, wy: float) -> np.ndarray:
+    rc = np.ascontiguousarray(rc, dtype=np.complex128)
+    Np, nfft = rc.shape
+    out = np.empty((nx, ny), dtype=np.complex128)
+    _check(lib().oracle_bp_ref64(Np, nfft, rc.view(np.float64).reshape(-1), *_geo(ax, ay, az, r0, f0),
+                                 float(max_wr), nx, ny, float(x0), float(y0), float(wx), float(wy),
+                                 out.view(np.float64).reshape(-1)), "bp_ref64")
+    return out
+
+
+def reference_focus(scene, precision: str = "f32", fast: bool = False, pulses: Optional[slice] = None):
+    """Run the reference's focus_SAR_image<T,T> (run_bp) on a scene.
+
+    Returns (image [nx, ny], max_Wy_m the reference derived, startF it used)."""
+    dtype = np.float32 if precision == "f32" else np.float64
+    ph, freq = pad_for_reference(scene, dtype)
+    sl = pulses if pulses is not None else slice(None)
+    ph = np.ascontiguousarray(ph[sl])
+    geo = [np.ascontiguousarray(v[sl], dtype=dtype) for v in (scene.ant_x, scene.ant_y, scene.ant_z,
+                                                              scene.slant_range)]
+    Np, nfft = ph.shape
+    g = scene.grid
+    img = np.empty((g.nx, g.ny), dtype=np.complex64 if dtype == np.float32 else np.complex128)
+    max_wy = np.zeros(1, dtype=dtype)
+    start_f = np.zeros(Np, dtype=dtype)
+    L = ref_lib(fast)
+    fn = L.ref_focus_bp_f32 if dtype == np.float32 else L.ref_focus_bp_f64
+    _check(fn(nfft, Np, ph.view(dtype).reshape(-1), freq, *geo, g.nx, g.ny, g.x0, g.y0, g.wx, g.wy,
+              img.view(dtype).reshape(-1), max_wy, start_f), "reference focus_SAR_image")
+    return img, float(max_wy[0]), start_f
+
+
+def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
+    a = np.asarray(a, dtype=np.complex128)
+    b = np.asarray(b, dtype=np.complex128)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+def peak_phase_error(a: np.ndarray, b: np.ndarray) -> float:
+    """Phase difference (rad) at the magnitude peak of b."""
+    b = np.asarray(b)
+    i = int(np.argmax(np.abs(b).ravel()))
+    return float(abs(np.angle(np.asarray(a).ravel()[i] * np.conj(b.ravel()[i]))))
