@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Backprojection throughput in pixel-pulses/s on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config large|point_targets]
+
+One step = range compression + backprojection of one synthetic aperture onto
+one image (sarbp_focus).  Default workload: the large mixed-precision
+configuration, 1024 frequency samples x 2048 pulses (complex64), fc 9.6 GHz,
+640 MHz, 30 deg of azimuth at 8 km and 45 deg elevation, 2000 Rayleigh
+scatterers, a 1024 x 1024 image over 100 m, Nfft = 8192 (2.15e9 pixel-pulses
+per step).  With N GPUs every rank forms its own 1024 x 1024 slab of a
+(1024 N) x 1024 image from the same aperture (weak scaling, no collective on
+the data path; the ranks only meet for the timing barrier and the max).
+
+Printed on rank 0 as one JSON line:
+  value     pixel-pulses/s over all ranks, inputs resident in HBM
+  e2e       the same through the C ABI with pinned host buffers: H2D of the
+            phase history and geometry, D2H of the image, every step
+  roofline  the backprojection kernel against the pipe that bounds it, with
+            per-pixel-pulse algorithmic work 10 FP64 + 16 FP32 flops,
+            2 transcendental (MUFU) ops and 16 B of on-chip gather, and the
+            pipe peaks measured by libsarbp_probes.so on this GPU in this run
+  cpu_baseline  the reference's own CPU backprojection (run_bp, compiled from
+            its sources into oracle/_ref) on a bounded pulse sample, all host
+            threads, rank 0 at N = 1
+--impl reference prints the reference CPU implementation's line alone.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BP pixel·pulses/s (mixed vs FP64, ≤1e-4 rel err); autofocus sec-to-focus"
+UNIT = "pixel·pulses/s"
+# algorithmic work per pixel-pulse (cpuBackProjection.hpp:65-87)
+WORK = {"fp64_flops": 10, "fp32_flops": 16, "sfu_ops": 2, "smem_bytes": 16}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=["large", "point_targets"], default="large")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
+    return ap.parse_args()
+
+
+def make_scene(config: str, rank: int, world: int, device):
+    from uncc_sar_focusing_b200 import scenes as S
+
+    if config == "large":
+        sc = S.large_scene(device=device)
+        desc = ("large: 1024 samples x 2048 pulses complex64, fc 9.6 GHz / 640 MHz, 30 deg at 8 km, 45 deg el, "
+                "2000 Rayleigh scatterers, 1024x1024 image over 100 m, Nfft 8192")
+        span = 100.0
+    else:
+        sc = S.point_target_scene(device=device)
+        desc = ("point_targets: 424 samples x 512 pulses complex64, fc 9.6 GHz / 600 MHz, 4 deg at 10 km, "
+                "30 deg el, 5 unit targets, 20 dB SNR, 256x256 image at 0.08 m, Nfft 3392")
+        span = sc.grid.wy + sc.grid.wy / (sc.grid.ny - 1)
+    # rank r takes slab r of an N-slab image along y
+    sc.grid.y0 = sc.grid.y0 + (rank - (world - 1) / 2.0) * span
+    return sc, desc
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", gpu_id, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference's run_bp (oracle/_ref) on a bounded pulse sample
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(scene, seconds: float, threads: int = 0):
+    """pixel-pulses/s of the reference CPU backprojection on this host, all
+    threads, each thread focusing its own slice of pulses (the operator is a
+    sum over pulses, so slices run side by side through the reference's
+    public focus_SAR_image call)."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    kind = "reference" if O.ref_available(fast=True) else "port"
+    threads = threads or os.cpu_count() or 1
+    npix = scene.grid.npix
+
+    def run(pulse_slices):
+        outs = [None] * len(pulse_slices)
+
+        def work(i, sl):
+            if kind == "reference":
+                outs[i] = O.reference_focus(scene, "f32", fast=True, pulses=sl)[0]
+            else:
+                ph, _ = O.pad_for_reference(scene, pulses=sl)
+                rc = O.range_compress_ref32(ph)
+                g = scene.grid
+                outs[i] = O.bp_ref32(rc, scene.ant_x[sl], scene.ant_y[sl], scene.ant_z[sl], scene.slant_range[sl],
+                                     scene.start_freq[sl], scene.max_wr, g.nx, g.ny, g.x0, g.y0, g.wx, g.wy)
+
+        ts = [threading.Thread(target=work, args=(i, sl)) for i, sl in enumerate(pulse_slices)]
+        t0 = time.perf_counter()
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        return time.perf_counter() - t0
+
+    Np = scene.num_pulses
+    # calibrate with two pulses per thread (the reference's aperture
+    # statistics need at least two pulses, uncc_sar_focusing.hpp:350-392)
+    t2 = run([slice(2 * i, 2 * i + 2) for i in range(min(threads, Np // 2))])
+    per_thread = max(2, min(Np // threads, int(2.0 * seconds / max(t2, 1e-3))))
+    stride = max(1, Np // (per_thread * threads))
+    slices = [slice(i * per_thread * stride, (i + 1) * per_thread * stride, stride) for i in range(threads)]
+    slices = [s for s in slices if s.start < Np]
+    total_pulses = sum(len(range(*s.indices(Np))) for s in slices)
+    dt = run(slices)
+    return {"value": npix * total_pulses / dt, "unit": UNIT, "cores": len(slices), "kind": kind,
+            "sample": f"{total_pulses} of {Np} pulses onto the full {scene.grid.nx}x{scene.grid.ny} grid, "
+                      f"{len(slices)} threads x {per_thread} pulses, {dt:.1f} s",
+            "seconds": dt}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sc, desc = make_scene(args.config, 0, 1, None if args.config != "large" else _scene_device())
+    per_step = max(2.0, 150.0 / max(1, args.steps + args.warmup))
+    vals = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        info = cpu_reference_rate(sc, per_step)
+        if i >= args.warmup:
+            vals.append(info["value"])
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": info["seconds"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": desc, "precision": "reference float (run_bp<float>)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
+                             "sample": info["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _scene_device():
+    try:
+        import torch
+
+        return "cuda" if torch.cuda.is_available() else None
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def probe_peaks():
+    from uncc_sar_focusing_b200 import build as B
+
+    L = ctypes.CDLL(B.PROBE_LIB)
+    L.sarbp_probe.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                              ctypes.POINTER(ctypes.c_float)]
+    out = {}
+    for which, name, iters, per_op in ((0, "fp32_flops_per_s", 4096, 2.0), (1, "fp64_flops_per_s", 2048, 2.0),
+                                       (2, "sfu_ops_per_s", 1024, 2.0), (3, "smem_bytes_per_s", 2048, 16.0)):
+        rate, ms = ctypes.c_double(), ctypes.c_float()
+        st = L.sarbp_probe(which, iters, ctypes.byref(rate), ctypes.byref(ms))
+        if st != 0:
+            raise RuntimeError(f"probe {name} failed: {st}")
+        out[name] = rate.value * per_op
+    return out
+
+
+def roofline_bound(peaks):
+    t = {"fp64": WORK["fp64_flops"] / peaks["fp64_flops_per_s"], "fp32": WORK["fp32_flops"] / peaks["fp32_flops_per_s"],
+         "sfu": WORK["sfu_ops"] / peaks["sfu_ops_per_s"], "smem": WORK["smem_bytes"] / peaks["smem_bytes_per_s"]}
+    bound = max(t, key=t.get)
+    return bound, 1.0 / t[bound], t
+
+
+def measured_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def gpu_arm(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from uncc_sar_focusing_b200 import focusing
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device(dev))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    sc, desc = make_scene(args.config, rank, world, dev)
+    pp = sc.pixel_pulses
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    ph_d = d(sc.phase_history)
+    geo_d = [d(v) for v in (sc.ant_x, sc.ant_y, sc.ant_z, sc.slant_range, sc.start_freq)]
+    plan = focusing.Plan.for_scene(sc, "mixed", device=local)
+    img_d = plan.new_image(dev)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, n):
+        barrier()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(n):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return a.elapsed_time(b)
+
+    step = lambda: plan.focus(ph_d, *geo_d, out=img_d)  # noqa: E731
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    plan.check()
+
+    props = torch.cuda.get_device_properties(local)
+    uuid = str(getattr(props, "uuid", ""))
+    gpu_id = uuid if uuid.startswith("GPU-") else (f"GPU-{uuid}" if uuid else str(local))
+    sampler = ClockSampler(gpu_id)
+    ms = timed(step, args.steps)
+    clocks = sampler.stop()
+    ms = max_over_ranks(ms)
+    ms_step = ms / args.steps
+    value = world * pp / (ms_step * 1e-3)
+
+    # kernel-level timings: range compression alone, backprojection alone
+    reps = max(3, args.steps)
+    rc_ms = max_over_ranks(timed(lambda: plan.range_compress(ph_d), reps)) / reps
+    plan.focus(ph_d, *geo_d, out=img_d)
+    bp_ms = max_over_ranks(timed(lambda: plan.backproject(*geo_d, out=img_d), reps)) / reps
+    plan.check()
+
+    # FP64 GPU path on the same inputs: accuracy reference and the FP64 baseline
+    img_mixed = img_d.clone()
+    plan64 = focusing.Plan.for_scene(sc, "fp64", device=local)
+    img64 = plan64.new_image(dev)
+    plan64.focus(ph_d, *geo_d, out=img64)
+    torch.cuda.synchronize()
+    plan64.check()
+    fp64_ms = max_over_ranks(timed(lambda: plan64.backproject(*geo_d, out=img64), max(2, args.steps // 3))) / max(
+        2, args.steps // 3)
+    diff = (img_mixed.to(torch.complex128) - img64).abs().pow(2).sum().sqrt()
+    rel = float(diff / img64.abs().pow(2).sum().sqrt())
+    del plan64, img64
+    torch.cuda.empty_cache()
+
+    # end to end through the C ABI with pinned host buffers
+    ph_h = torch.empty(ph_d.shape, dtype=ph_d.dtype, pin_memory=True)
+    ph_h.copy_(ph_d.cpu())
+    geo_h = []
+    for v in geo_d:
+        h = torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
+        h.copy_(v.cpu())
+        geo_h.append(h)
+    img_h = torch.empty(img_d.shape, dtype=img_d.dtype, pin_memory=True)
+    ph_n, geo_n, img_n = ph_h.numpy(), [g.numpy() for g in geo_h], img_h.numpy()
+    e2e_step = lambda: plan.focus(ph_n, *geo_n, out=img_n)  # noqa: E731
+    for _ in range(2):
+        e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = max_over_ranks(time.perf_counter() - t0) / args.steps
+    h2d = ph_n.nbytes + sum(g.nbytes for g in geo_n)
+    d2h = img_n.nbytes
+    assert np.allclose(img_n, img_mixed.cpu().numpy(), rtol=0, atol=1e-6 * float(np.abs(img_n).max()))
+
+    line = None
+    if rank == 0:
+        peaks = probe_peaks()
+        bound, roof, tmin = roofline_bound(peaks)
+        bp_rate = pp / (bp_ms * 1e-3)
+        hbm, hbm_kind = measured_hbm()
+        rc_bytes = sc.num_pulses * (sc.num_range_samples * 8 + sc.nfft * 8)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64 (FP64 per-tile geometry, FP32 per pixel-pulse)",
+            "data": "synthetic",
+            "config": {"workload": desc, "pixels_per_gpu": sc.grid.npix, "pulses": sc.num_pulses,
+                       "range_samples": sc.num_range_samples, "nfft": sc.nfft, "precision": "mixed",
+                       "pixel_pulses_per_step_per_gpu": pp,
+                       "l2": "inputs larger than L2 (range-profile pair buffer "
+                             f"{plan.workspace_bytes / 2**20:.0f} MiB plan workspace)",
+                       "parallelism": f"{world} image slab(s), one per GPU, no data-path collective"},
+            "accuracy": {"rel_l2_mixed_vs_fp64_gpu": rel, "tolerance": 1e-4},
+            "fp64_gpu": {"bp_value": pp / (fp64_ms * 1e-3), "unit": UNIT,
+                         "mixed_speedup": (pp / (bp_ms * 1e-3)) / (pp / (fp64_ms * 1e-3))},
+            "e2e": {"value": world * pp / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": 3 * args.steps,
+            "kernels": {"bp_ms": bp_ms, "range_compress_ms": rc_ms,
+                        "range_compress_hbm": {"bytes": rc_bytes, "achieved_gbs": rc_bytes / (rc_ms * 1e-3) / 1e9,
+                                               "peak_gbs": hbm, "peak_kind": hbm_kind,
+                                               "frac": rc_bytes / (rc_ms * 1e-3) / 1e9 / hbm}},
+            "roofline": {"bound": bound, "achieved": bp_rate, "peak": roof, "unit": UNIT, "frac": bp_rate / roof,
+                         "traffic": None, "peak_kind": "measured in this run by libsarbp_probes.so",
+                         "work_per_pixel_pulse": WORK, "pipe_peaks": peaks,
+                         "t_min_per_pixel_pulse_s": tmin},
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            cb = cpu_reference_rate(sc, args.cpu_seconds)
+            cb.pop("seconds", None)
+            line["cpu_baseline"] = cb
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,183 @@
+/*
+ * sarbp.h -- C ABI of the B200 (sm_100a) SAR backprojection engine.
+ *
+ * The engine replaces the reference's GPU focusing call
+ *
+ *     template <typename T, typename P>
+ *     void cuda_focus_SAR_image(const SAR_Aperture<T>&,
+ *                               const SAR_ImageFormationParameters<P>&,
+ *                               CArray<T>& output_image);
+ *
+ * (src/gpuBackProjection/cuda_sar_focusing/cuda_sar_focusing.hpp:526-723,
+ * declared include/charlotte_sar_api.hpp:256-259, exported as the
+ * <float,float> and <double,double> instantiations of
+ * libuncc_sar_focusing_gpu.so, src/gpuBackProjection/cuda_sar_focusing/
+ * libcuda_sar_focusing.cu:26-32).  That call is one monolithic step: copy
+ * the aperture to the GPU, batched inverse FFT (:616-617), 1/N scaling
+ * (:618), fftshift (:620), backprojection kernel (:659-670), copy back.
+ * Here the same step is split into a reusable plan (device buffers and the
+ * FFT plan are created once) and entry points for range compression,
+ * backprojection, both together, and the adjoint.  A C++ shim that exports
+ * the reference's own template symbols on top of this ABI is built as
+ * libsarbp_compat.so.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (SARBP_OK == 0).  Nothing calls
+ *    cudaDeviceReset() (the reference does, cuda_sar_focusing.hpp:516).
+ *  - Complex data are interleaved (re, im) pairs: complex64 = 2 x float,
+ *    complex128 = 2 x double.
+ *  - Phase history: complex64 [num_pulses][num_range_samples], frequency
+ *    fastest, i.e. SAR_Aperture::sampleData (include/uncc_sar_focusing.hpp:68).
+ *  - Images: [nz][nx][ny], x-major inside a z-slice: pixel (ix, iy) at
+ *    ix*ny + iy as cpuBackProjection.hpp:87 / cuda_BackProjectionKernels.cuh:
+ *    91-92.  complex64 for SARBP_PRECISION_MIXED, complex128 for
+ *    SARBP_PRECISION_FP64.
+ *  - Pixel ix sits at x0 - wx/2 + ix * wx/(nx-1) (cpuBackProjection.hpp:
+ *    55-62); likewise y and z.  nz == 1 is the plane z = z0.
+ *  - Stream arguments are cudaStream_t passed as void* (NULL = legacy stream).
+ *  - Pointers flagged SARBP_MEMORY_HOST are ordinary host memory; calls that
+ *    take or return host memory synchronise the stream before returning.
+ *    Calls on device memory are asynchronous; sarbp_plan_check() reads back
+ *    kernel-side error flags.
+ */
+#ifndef SARBP_H
+#define SARBP_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SARBP_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define SARBP_API __attribute__((visibility("default")))
+#else
+#define SARBP_API
+#endif
+
+/* Status codes */
+enum {
+    SARBP_OK = 0,
+    SARBP_ERR_INVALID_ARGUMENT = 1, /* a size, flag or grid value is out of range */
+    SARBP_ERR_NULL_POINTER = 2,     /* a required pointer is NULL */
+    SARBP_ERR_UNSUPPORTED = 3,      /* valid request this build cannot serve */
+    SARBP_ERR_OUT_OF_MEMORY = 4,    /* a device or host allocation failed */
+    SARBP_ERR_CUDA = 5,             /* a CUDA runtime call failed */
+    SARBP_ERR_CUFFT = 6,            /* a cuFFT call failed */
+    SARBP_ERR_NOT_FINITE = 7,       /* non-finite geometry reached a kernel */
+    SARBP_ERR_KERNEL_TIMEOUT = 8,   /* a bounded device wait gave up */
+    SARBP_ERR_KERNEL_BOUNDS = 9,    /* a checked kernel clamped an index */
+    SARBP_ERR_NO_DEVICE = 10        /* no CUDA device available */
+};
+
+/* Arithmetic of the backprojection */
+enum {
+    /* FP64 per-tile geometry and phase reduction, FP32 interpolation,
+     * rotation and accumulation; complex64 image. */
+    SARBP_PRECISION_MIXED = 0,
+    /* everything in FP64 (range compression, geometry, interpolation,
+     * rotation, accumulation); complex128 image. */
+    SARBP_PRECISION_FP64 = 1
+};
+
+/* Range taper applied before zero padding */
+enum {
+    SARBP_WINDOW_NONE = 0,
+    SARBP_WINDOW_HAMMING = 1 /* 0.54 - 0.46 cos(2 pi k / (K-1)) */
+};
+
+/* Where a pointer lives */
+enum { SARBP_MEMORY_HOST = 0, SARBP_MEMORY_DEVICE = 1 };
+
+/* sarbp_backproject flags */
+enum {
+    SARBP_ACCUMULATE = 1, /* add into the image instead of overwriting it */
+    SARBP_CHECKED = 2     /* bounds-checked kernel variant (tests) */
+};
+
+/* Image grid (SAR_ImageFormationParameters N_x_pix, N_y_pix, x0_m, y0_m,
+ * Wx_m, Wy_m, include/uncc_sar_focusing.hpp:405-412, plus a z axis). */
+typedef struct sarbp_grid {
+    int nx, ny, nz;
+    double x0, y0, z0;
+    double wx, wy, wz;
+} sarbp_grid;
+
+typedef struct sarbp_plan_desc {
+    int num_range_samples; /* K: frequency samples per pulse */
+    int num_pulses;        /* Np: pulses per call (upper bound) */
+    int nfft;              /* FFT length >= K (SAR_ImageFormationParameters::N_fft) */
+    double max_wr;         /* range-profile extent in metres, c/(2 dF)
+                              (SAR_ImageFormationParameters::max_Wy_m, :429) */
+    sarbp_grid grid;
+    int precision;         /* SARBP_PRECISION_* */
+    int window;            /* SARBP_WINDOW_* */
+    int device;            /* CUDA ordinal, -1 = current device */
+    int reserved[4];       /* zero */
+} sarbp_plan_desc;
+
+/* Per-pulse geometry: antenna phase centre (Ant_x/y/z), slant range to the
+ * scene centre R0 (slant_range) and start frequency f0 (startF), all double
+ * [num_pulses] (SAR_Aperture, include/uncc_sar_focusing.hpp:69-87). */
+typedef struct sarbp_geometry {
+    const double *ant_x, *ant_y, *ant_z;
+    const double *slant_range;
+    const double *start_freq;
+    int num_pulses;
+    int memory; /* SARBP_MEMORY_* for all five arrays */
+} sarbp_geometry;
+
+typedef struct sarbp_aperture {
+    const void *phase_history; /* complex64 [num_pulses][K] */
+    int phase_history_memory;  /* SARBP_MEMORY_* */
+    sarbp_geometry geometry;
+} sarbp_aperture;
+
+typedef struct sarbp_plan sarbp_plan;
+
+SARBP_API int sarbp_abi_version(void);
+SARBP_API const char *sarbp_status_string(int status);
+
+/* Create / destroy a plan.  All device memory and the FFT plan are created
+ * here (GPUMemoryManager + cufft_engine, cuda_sar_focusing.hpp:93-348,372-399,
+ * done once instead of per call). */
+SARBP_API int sarbp_plan_create(const sarbp_plan_desc *desc, sarbp_plan **plan);
+SARBP_API int sarbp_plan_destroy(sarbp_plan *plan);
+/* Device bytes the plan holds. */
+SARBP_API int sarbp_plan_workspace_bytes(const sarbp_plan *plan, size_t *bytes);
+
+/* Range compression (cuda_sar_focusing.hpp:616-620 plus the zero pad and
+ * taper of matlab/bpBasic.m:82, matlab/formImage3DSAR.m:115-116):
+ *   rc_p = fftshift(ifft(w .* ph_p, nfft)) for every pulse,
+ * kept inside the plan for the next sarbp_backproject. */
+SARBP_API int sarbp_range_compress(sarbp_plan *plan, const void *phase_history, int num_pulses, int memory,
+                         void *stream);
+
+/* Copy the plan's range profiles out: complex64 (MIXED) or complex128 (FP64)
+ * [num_pulses][nfft]. */
+SARBP_API int sarbp_get_range_profiles(sarbp_plan *plan, void *out, int memory, void *stream);
+
+/* Backprojection of the plan's range profiles onto the grid
+ * (cuda_BackProjectionKernels.cuh:33-93, cpuBackProjection.hpp:49-93). */
+SARBP_API int sarbp_backproject(sarbp_plan *plan, const sarbp_geometry *geometry, void *image, int image_memory,
+                      int flags, void *stream);
+
+/* Range compression + backprojection: the reference's cuda_focus_SAR_image. */
+SARBP_API int sarbp_focus(sarbp_plan *plan, const sarbp_aperture *aperture, void *image, int image_memory,
+                void *stream);
+
+/* One call, no plan kept: create, focus, destroy (host or device buffers). */
+SARBP_API int sarbp_focus_image(const sarbp_plan_desc *desc, const sarbp_aperture *aperture, void *image,
+                      int image_memory);
+
+/* Synchronise the stream, read and clear the plan's device error flags and
+ * return the first error they record (SARBP_OK if none). */
+SARBP_API int sarbp_plan_check(sarbp_plan *plan, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SARBP_H */

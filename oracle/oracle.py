@@ -155,15 +155,15 @@ def focus_fp64(scene, pixels: Optional[np.ndarray] = None) -> np.ndarray:
     return bp_fp64_pixels(*args, pixels)
 
 
-def pad_for_reference(scene, dtype=np.float32):
+def pad_for_reference(scene, dtype=np.float32, pulses: Optional[slice] = None):
     """The reference has no zero pad or window (cpuBackProjection.hpp:107-110):
     feed it w.*ph zero-padded from K to Nfft and freq extended at the same step."""
     K = scene.num_range_samples
     w = window_for(scene.window, K)
-    ph = scene.phase_history.astype(np.complex128)
+    ph = scene.phase_history[pulses if pulses is not None else slice(None)].astype(np.complex128)
     if w is not None:
         ph = ph * w[None, :]
-    padded = np.zeros((scene.num_pulses, scene.nfft), dtype=np.complex128)
+    padded = np.zeros((ph.shape[0], scene.nfft), dtype=np.complex128)
     padded[:, :K] = ph
     freq = scene.start_freq[0] + np.arange(scene.nfft, dtype=np.float64) * scene.delta_freq
     ctype = np.complex64 if dtype == np.float32 else np.complex128
@@ -216,9 +216,9 @@ def reference_focus(scene, precision: str = "f32", fast: bool = False, pulses: O
 
     Returns (image [nx, ny], max_Wy_m the reference derived, startF it used)."""
     dtype = np.float32 if precision == "f32" else np.float64
-    ph, freq = pad_for_reference(scene, dtype)
     sl = pulses if pulses is not None else slice(None)
-    ph = np.ascontiguousarray(ph[sl])
+    ph, freq = pad_for_reference(scene, dtype, sl)
+    ph = np.ascontiguousarray(ph)
     geo = [np.ascontiguousarray(v[sl], dtype=dtype) for v in (scene.ant_x, scene.ant_y, scene.ant_z,
                                                               scene.slant_range)]
     Np, nfft = ph.shape

@@ -19,15 +19,23 @@
 
 #include <cstring>
 #include <iostream>
+#include <mutex>
 
 #include <cpuBackProjection.hpp>
 
 namespace {
 
+// The reference prints progress to std::cout and its FILE logger on every
+// call.  Both are switched off once per process (never toggled back, so calls
+// from several threads at once do not race on the stream state).
 struct QuietReference {
-    std::streambuf *saved;
-    QuietReference() : saved(std::cout.rdbuf(nullptr)) { Output2FILE::Stream() = nullptr; }
-    ~QuietReference() { std::cout.rdbuf(saved); }
+    QuietReference() {
+        static std::once_flag once;
+        std::call_once(once, [] {
+            std::cout.rdbuf(nullptr);
+            Output2FILE::Stream() = nullptr;
+        });
+    }
 };
 
 template <typename T>

@@ -1,0 +1,187 @@
+"""GPU parity of the range compression and backprojection kernels against the
+FP64 oracle, through the C ABI (libsarbp.so via uncc_sar_focusing_b200.focusing).
+
+Tolerances: the mixed-precision path must stay within 1e-4 relative L2 of the
+FP64 oracle image (the stated accuracy target), the FP64 path within 1e-10.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from uncc_sar_focusing_b200 import scenes as S
+
+pytestmark = pytest.mark.gpu
+
+MIXED_TOL = 1e-4
+FP64_TOL = 1e-10
+
+
+@pytest.fixture(scope="module")
+def F():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from uncc_sar_focusing_b200 import focusing
+
+    return focusing
+
+
+def small_scene(**kw):
+    args = dict(K=64, Np=48, n=40, spacing=0.2, nfft=512, snr_db=20.0, seed=3, n_targets=4, extent=6.0)
+    args.update(kw)
+    return S.point_target_scene(**args)
+
+
+@pytest.mark.parametrize("precision,tol", [("mixed", 2e-6), ("fp64", 1e-13)])
+def test_range_compression_matches_oracle(F, precision, tol):
+    sc = small_scene(K=53, nfft=424)
+    with F.Plan.for_scene(sc, precision) as plan:
+        plan.range_compress(sc.phase_history)
+        got = plan.range_profiles()
+    want = O.range_compress_fp64(sc.phase_history, sc.nfft, O.hamming(sc.num_range_samples))
+    assert O.rel_l2(got, want) < tol
+
+
+@pytest.mark.parametrize("nfft", [256, 255, 424])
+def test_range_compression_odd_and_mixed_radix_lengths(F, nfft):
+    sc = small_scene(K=40, nfft=nfft)
+    sc.window = "none"
+    with F.Plan.for_scene(sc, "mixed") as plan:
+        plan.range_compress(sc.phase_history)
+        got = plan.range_profiles()
+    want = O.range_compress_fp64(sc.phase_history, nfft, None)
+    assert O.rel_l2(got, want) < 2e-6
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_focus_small_scene(F, precision):
+    sc = small_scene()
+    want = O.focus_fp64(sc)
+    got = F.focus_scene(sc, precision)
+    err = O.rel_l2(got, want)
+    assert err < (MIXED_TOL if precision == "mixed" else FP64_TOL), err
+    assert np.isfinite(got).all()
+
+
+def test_point_target_config_full_image(F):
+    # the point-target configuration: 424 x 512, 5 targets, 20 dB SNR, 256^2 at 0.08 m, Nfft = 8K
+    sc = S.point_target_scene()
+    want = O.focus_fp64(sc)
+    got = F.focus_scene(sc, "mixed")
+    err = O.rel_l2(got, want)
+    assert err < MIXED_TOL, err
+    assert O.peak_phase_error(got, want) < 1e-3
+    got64 = F.focus_scene(sc, "fp64")
+    assert O.rel_l2(got64, want) < FP64_TOL
+
+
+def test_golden_cases_match_reference_double_path(F):
+    import golden_cases as G
+
+    for name in G.names():
+        sc, d = G.load(name)
+        got = F.focus_scene(sc, "fp64")[0]
+        # run_bp<double> keeps dR in float; the oracle tests bound the same gap
+        assert O.rel_l2(got, d["ref_img_f64"]) < 3e-4
+        assert O.rel_l2(got, O.focus_fp64(sc)[0]) < FP64_TOL
+
+
+def test_grid_edges_odd_sizes_and_offsets(F):
+    sc = small_scene()
+    sc.grid = S.Grid(nx=37, ny=45, x0=0.7, y0=-0.4, wx=36 * 0.17, wy=44 * 0.21)
+    want = O.focus_fp64(sc)
+    for precision, tol in (("mixed", MIXED_TOL), ("fp64", FP64_TOL)):
+        got = F.focus_scene(sc, precision)
+        assert O.rel_l2(got, want) < tol
+
+
+def test_swath_edges_are_gated_like_the_reference(F):
+    # a grid far larger than the unambiguous range swath: pixels beyond
+    # rmin/rmax must get no contribution, exactly as the oracle's strict gate
+    sc = small_scene(K=32, nfft=64, n=8, spacing=1.0)
+    sc.grid = S.Grid(nx=70, ny=45, wx=69 * 0.9, wy=44 * 1.3, x0=3.0, y0=-2.0)
+    want = O.focus_fp64(sc)
+    got = F.focus_scene(sc, "mixed")
+    assert O.rel_l2(got, want) < MIXED_TOL
+    got64 = F.focus_scene(sc, "fp64")
+    assert O.rel_l2(got64, want) < FP64_TOL
+
+
+def test_near_field_geometry_takes_the_exact_path(F):
+    sc = small_scene(radius=60.0, spacing=0.1, n=64)
+    want = O.focus_fp64(sc)
+    got = F.focus_scene(sc, "mixed")
+    assert O.rel_l2(got, want) < MIXED_TOL
+
+
+def test_volume_grid(F):
+    sc = small_scene(n=24)
+    sc.grid = S.Grid(nx=24, ny=30, nz=5, wx=23 * 0.2, wy=29 * 0.2, wz=2.0, z0=0.3)
+    want = O.focus_fp64(sc)
+    got = F.focus_scene(sc, "mixed")
+    assert got.shape == (5, 24, 30)
+    assert O.rel_l2(got, want) < MIXED_TOL
+
+
+def test_device_pointers_match_host_pointers_and_accumulate(F):
+    import torch
+
+    sc = small_scene()
+    host = F.focus_scene(sc, "mixed")
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    with F.Plan.for_scene(sc, "mixed") as plan:
+        img = plan.focus(dev(sc.phase_history), dev(sc.ant_x), dev(sc.ant_y), dev(sc.ant_z),
+                         dev(sc.slant_range), dev(sc.start_freq))
+        torch.cuda.synchronize()
+        plan.check()
+        assert np.array_equal(img.cpu().numpy(), host)
+        # two halves of the aperture accumulated == the whole aperture (linearity in pulses)
+        h = sc.num_pulses // 2
+        out = plan.new_image("cuda")
+        for sl in (slice(0, h), slice(h, None)):
+            plan.range_compress(dev(sc.phase_history[sl]))
+            plan.backproject(*(dev(v[sl]) for v in (sc.ant_x, sc.ant_y, sc.ant_z, sc.slant_range, sc.start_freq)),
+                             out=out, accumulate=True)
+        torch.cuda.synchronize()
+        assert O.rel_l2(out.cpu().numpy(), host) < 1e-6
+
+
+def test_checked_kernel_records_no_out_of_range_index(F):
+    import torch
+
+    sc = small_scene()
+    sc.grid = S.Grid(nx=70, ny=45, wx=69 * 0.5, wy=44 * 0.7)
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    with F.Plan.for_scene(sc, "mixed") as plan:
+        plan.range_compress(dev(sc.phase_history))
+        img = plan.backproject(*(dev(v) for v in (sc.ant_x, sc.ant_y, sc.ant_z, sc.slant_range, sc.start_freq)),
+                               checked=True)
+        plan.check()  # raises SarbpError on SARBP_ERR_KERNEL_BOUNDS
+    assert O.rel_l2(img.cpu().numpy(), O.focus_fp64(sc)) < MIXED_TOL
+
+
+def test_non_finite_geometry_is_reported(F):
+    sc = small_scene()
+    ax = sc.ant_x.copy()
+    ax[3] = np.nan
+    with F.Plan.for_scene(sc, "mixed") as plan:
+        with pytest.raises(F.N.SarbpError) as ei:
+            plan.focus(sc.phase_history, ax, sc.ant_y, sc.ant_z, sc.slant_range, sc.start_freq)
+        assert ei.value.status == F.N.SARBP_ERR_NOT_FINITE
+
+
+def test_large_config_sampled_pixels(F):
+    # the large configuration at full size: 1024 samples x 2048 pulses, 2000
+    # Rayleigh scatterers, 1024^2 over 100 m; checked on 3000 pixels
+    import torch
+
+    sc = S.large_scene(device="cuda")
+    img = F.focus_scene(sc, "mixed")
+    rng = np.random.default_rng(0)
+    pix = np.sort(rng.choice(img.size, 3000, replace=False))
+    want = O.focus_fp64(sc, pixels=pix)
+    got = img.reshape(-1)[pix]
+    assert O.rel_l2(got, want) < MIXED_TOL
+    assert np.isfinite(img).all()
+    torch.cuda.empty_cache()

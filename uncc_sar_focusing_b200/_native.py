@@ -1,0 +1,105 @@
+"""ctypes binding of lib/libsarbp.so (include/sarbp.h).
+
+The library is the product: there is no Python or CPU fallback.  Loading
+fails with a RuntimeError when it has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libsarbp.so")
+COMPAT_PATH = os.path.join(HERE, "lib", "libsarbp_compat.so")
+
+SARBP_OK = 0
+SARBP_ERR_INVALID_ARGUMENT = 1
+SARBP_ERR_NULL_POINTER = 2
+SARBP_ERR_UNSUPPORTED = 3
+SARBP_ERR_OUT_OF_MEMORY = 4
+SARBP_ERR_CUDA = 5
+SARBP_ERR_CUFFT = 6
+SARBP_ERR_NOT_FINITE = 7
+SARBP_ERR_KERNEL_TIMEOUT = 8
+SARBP_ERR_KERNEL_BOUNDS = 9
+SARBP_ERR_NO_DEVICE = 10
+
+PRECISION_MIXED = 0
+PRECISION_FP64 = 1
+WINDOW_NONE = 0
+WINDOW_HAMMING = 1
+MEMORY_HOST = 0
+MEMORY_DEVICE = 1
+ACCUMULATE = 1
+CHECKED = 2
+
+# Every symbol include/sarbp.h declares (tests check the library exports them).
+EXPORTED = (
+    "sarbp_abi_version", "sarbp_status_string", "sarbp_plan_create", "sarbp_plan_destroy",
+    "sarbp_plan_workspace_bytes", "sarbp_range_compress", "sarbp_get_range_profiles", "sarbp_backproject",
+    "sarbp_focus", "sarbp_focus_image", "sarbp_plan_check",
+)
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("x0", ctypes.c_double), ("y0", ctypes.c_double), ("z0", ctypes.c_double),
+                ("wx", ctypes.c_double), ("wy", ctypes.c_double), ("wz", ctypes.c_double)]
+
+
+class PlanDesc(ctypes.Structure):
+    _fields_ = [("num_range_samples", ctypes.c_int), ("num_pulses", ctypes.c_int), ("nfft", ctypes.c_int),
+                ("max_wr", ctypes.c_double), ("grid", Grid), ("precision", ctypes.c_int),
+                ("window", ctypes.c_int), ("device", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
+
+
+class Geometry(ctypes.Structure):
+    _fields_ = [("ant_x", ctypes.c_void_p), ("ant_y", ctypes.c_void_p), ("ant_z", ctypes.c_void_p),
+                ("slant_range", ctypes.c_void_p), ("start_freq", ctypes.c_void_p),
+                ("num_pulses", ctypes.c_int), ("memory", ctypes.c_int)]
+
+
+class Aperture(ctypes.Structure):
+    _fields_ = [("phase_history", ctypes.c_void_p), ("phase_history_memory", ctypes.c_int),
+                ("geometry", Geometry)]
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m uncc_sar_focusing_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i, P = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER
+        L.sarbp_abi_version.restype = i
+        L.sarbp_status_string.restype = ctypes.c_char_p
+        L.sarbp_status_string.argtypes = [i]
+        L.sarbp_plan_create.argtypes = [P(PlanDesc), P(vp)]
+        L.sarbp_plan_destroy.argtypes = [vp]
+        L.sarbp_plan_workspace_bytes.argtypes = [vp, P(ctypes.c_size_t)]
+        L.sarbp_range_compress.argtypes = [vp, vp, i, i, vp]
+        L.sarbp_get_range_profiles.argtypes = [vp, vp, i, vp]
+        L.sarbp_backproject.argtypes = [vp, P(Geometry), vp, i, i, vp]
+        L.sarbp_focus.argtypes = [vp, P(Aperture), vp, i, vp]
+        L.sarbp_focus_image.argtypes = [P(PlanDesc), P(Aperture), vp, i]
+        L.sarbp_plan_check.argtypes = [vp, vp]
+        for name in EXPORTED:
+            if name != "sarbp_status_string":
+                getattr(L, name).restype = i
+        _LIB = L
+    return _LIB
+
+
+class SarbpError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        msg = lib().sarbp_status_string(status).decode()
+        super().__init__(f"{what}: {msg} (status {status})")
+
+
+def check(status: int, what: str) -> None:
+    if status != SARBP_OK:
+        raise SarbpError(status, what)

@@ -1,0 +1,486 @@
+// api.cu -- the C ABI of include/sarbp.h.
+//
+// Host-side driver in place of the reference's cuda_focus_SAR_image
+// (src/gpuBackProjection/cuda_sar_focusing/cuda_sar_focusing.hpp:526-723):
+// plan creation holds what the reference re-creates on every call
+// (GPUMemoryManager allocations :93-348, the cuFFT plan :372-399, the range
+// bin vector :574-598), every call is stream-ordered, errors come back as
+// status codes, and nothing resets the device.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "bp_common.cuh"
+#include "sarbp_internal.h"
+
+using namespace sarbp;
+
+namespace {
+
+int from_cuda(cudaError_t e) {
+    if (e == cudaSuccess) return SARBP_OK;
+    if (e == cudaErrorMemoryAllocation) return SARBP_ERR_OUT_OF_MEMORY;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return SARBP_ERR_NO_DEVICE;
+    return SARBP_ERR_CUDA;
+}
+
+int from_cufft(cufftResult r) {
+    if (r == CUFFT_SUCCESS) return SARBP_OK;
+    if (r == CUFFT_ALLOC_FAILED) return SARBP_ERR_OUT_OF_MEMORY;
+    return SARBP_ERR_CUFFT;
+}
+
+#define SARBP_TRY_CUDA(call)                  \
+    do {                                      \
+        const cudaError_t e_ = (call);        \
+        if (e_ != cudaSuccess) {              \
+            cudaGetLastError();               \
+            return from_cuda(e_);             \
+        }                                     \
+    } while (0)
+
+// Makes plan->device current for the duration of a call and restores the
+// caller's device afterwards.
+struct DeviceGuard {
+    int prev = -1;
+    bool changed = false;
+    cudaError_t status = cudaSuccess;
+    explicit DeviceGuard(int dev) {
+        status = cudaGetDevice(&prev);
+        if (status == cudaSuccess && prev != dev) {
+            status = cudaSetDevice(dev);
+            changed = status == cudaSuccess;
+        }
+    }
+    ~DeviceGuard() {
+        if (changed) cudaSetDevice(prev);
+    }
+};
+
+bool finite_nonneg(double v) { return std::isfinite(v) && v >= 0.0; }
+
+int validate_desc(const sarbp_plan_desc *d) {
+    if (!d) return SARBP_ERR_NULL_POINTER;
+    const sarbp_grid &g = d->grid;
+    if (d->num_range_samples < 1 || d->num_pulses < 1 || d->nfft < 2 || d->nfft < d->num_range_samples ||
+        d->nfft > (1 << 24))
+        return SARBP_ERR_INVALID_ARGUMENT;
+    if (!(std::isfinite(d->max_wr) && d->max_wr > 0.0)) return SARBP_ERR_INVALID_ARGUMENT;
+    if (g.nx < 1 || g.ny < 1 || g.nz < 1 || g.nx > (1 << 20) || g.ny > (1 << 20) || g.nz > 65535)
+        return SARBP_ERR_INVALID_ARGUMENT;
+    if (!(std::isfinite(g.x0) && std::isfinite(g.y0) && std::isfinite(g.z0) && finite_nonneg(g.wx) &&
+          finite_nonneg(g.wy) && finite_nonneg(g.wz)))
+        return SARBP_ERR_INVALID_ARGUMENT;
+    if (d->precision != SARBP_PRECISION_MIXED && d->precision != SARBP_PRECISION_FP64)
+        return SARBP_ERR_INVALID_ARGUMENT;
+    if (d->window != SARBP_WINDOW_NONE && d->window != SARBP_WINDOW_HAMMING) return SARBP_ERR_INVALID_ARGUMENT;
+    const double samples = static_cast<double>(d->num_pulses) * static_cast<double>(d->nfft);
+    if (samples > 4.0e9) return SARBP_ERR_UNSUPPORTED;
+    return SARBP_OK;
+}
+
+void axis(int n, double c, double w, double *lo, double *step) {
+    if (n > 1) {
+        *step = w / static_cast<double>(n - 1);
+        *lo = c - 0.5 * w;
+    } else {
+        *step = 0.0;
+        *lo = c;
+    }
+}
+
+// Window geometry for a tile of (8*mx) x 64 pixels centred on an integer pixel.
+void window_for(const sarbp_plan *p, int mx, int *W, int *wsize) {
+    const double hx = 0.5 * 8.0 * mx * p->dx, hy = 0.5 * 64.0 * p->dy;
+    const double hd = std::sqrt(hx * hx + hy * hy);
+    *W = static_cast<int>(std::ceil(p->lambda * hd)) + 3;
+    *wsize = 2 * (*W) + 2;
+}
+
+// Largest stage depth whose shared memory fits 2 CTAs per SM (mixed) or one
+// (FP64); environment SARBP_TILE="mx,pb" overrides (tuning runs).
+int choose_tile(sarbp_plan *p) {
+    static const int cand_mixed[][2] = {{4, 8}, {4, 4}, {2, 8}, {2, 4}, {1, 8}};
+    static const int cand_fp64[][2] = {{4, 4}, {2, 4}, {1, 8}};
+    const bool fp64 = p->precision == SARBP_PRECISION_FP64;
+    const size_t limit = fp64 ? 220u * 1024u : 110u * 1024u;
+    int forced_mx = 0, forced_pb = 0;
+    if (const char *env = std::getenv("SARBP_TILE")) {
+        if (std::sscanf(env, "%d,%d", &forced_mx, &forced_pb) != 2) forced_mx = forced_pb = 0;
+    }
+    const int n = fp64 ? 3 : 5;
+    for (int i = -1; i < n; ++i) {
+        int mx, pb;
+        if (i < 0) {
+            if (!forced_mx) continue;
+            mx = forced_mx;
+            pb = forced_pb;
+        } else {
+            mx = fp64 ? cand_fp64[i][0] : cand_mixed[i][0];
+            pb = fp64 ? cand_fp64[i][1] : cand_mixed[i][1];
+        }
+        int W, wsize;
+        window_for(p, mx, &W, &wsize);
+        if (wsize > (1 << 16)) continue;
+        TileConfig tc{mx, pb};
+        const size_t smem = fp64 ? bp_fp64_smem_bytes(tc, wsize) : bp_mixed_smem_bytes(tc, wsize);
+        if (smem > (i < 0 ? 227u * 1024u : limit)) continue;
+        p->tile = tc;
+        p->W = W;
+        p->wsize = wsize;
+        p->smem = smem;
+        return SARBP_OK;
+    }
+    return SARBP_ERR_UNSUPPORTED;
+}
+
+void release(sarbp_plan *p) {
+    if (!p) return;
+    if (p->fft_ok) cufftDestroy(p->fft);
+    cudaFree(p->d_ph);
+    cudaFree(p->d_geo);
+    cudaFree(p->d_fft);
+    cudaFree(p->d_pairs);
+    cudaFree(p->d_fac);
+    cudaFree(p->d_img);
+    cudaFree(p->d_err);
+    delete p;
+}
+
+int alloc(sarbp_plan *p, void **ptr, size_t bytes) {
+    const cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *ptr = nullptr;
+        return from_cuda(e);
+    }
+    p->bytes += bytes;
+    return SARBP_OK;
+}
+
+size_t cplx_bytes(const sarbp_plan *p) { return p->precision == SARBP_PRECISION_FP64 ? 16 : 8; }
+
+int check_geometry_host(const sarbp_geometry *g) {
+    const double *arrs[5] = {g->ant_x, g->ant_y, g->ant_z, g->slant_range, g->start_freq};
+    for (const double *a : arrs)
+        for (int i = 0; i < g->num_pulses; ++i)
+            if (!std::isfinite(a[i])) return SARBP_ERR_NOT_FINITE;
+    return SARBP_OK;
+}
+
+int read_errors(sarbp_plan *p, cudaStream_t s) {
+    SARBP_TRY_CUDA(cudaStreamSynchronize(s));
+    unsigned bits = 0;
+    SARBP_TRY_CUDA(cudaMemcpy(&bits, p->d_err, sizeof(bits), cudaMemcpyDeviceToHost));
+    if (bits) SARBP_TRY_CUDA(cudaMemset(p->d_err, 0, sizeof(unsigned)));
+    if (bits & ERRBIT_TIMEOUT) return SARBP_ERR_KERNEL_TIMEOUT;
+    if (bits & ERRBIT_NOT_FINITE) return SARBP_ERR_NOT_FINITE;
+    if (bits & ERRBIT_BOUNDS) return SARBP_ERR_KERNEL_BOUNDS;
+    return SARBP_OK;
+}
+
+int range_compress_impl(sarbp_plan *p, const void *ph, int np, int memory, cudaStream_t s) {
+    if (!ph) return SARBP_ERR_NULL_POINTER;
+    if (np < 1 || np > p->np_cap) return SARBP_ERR_INVALID_ARGUMENT;
+    if (memory != SARBP_MEMORY_HOST && memory != SARBP_MEMORY_DEVICE) return SARBP_ERR_INVALID_ARGUMENT;
+    const void *src = ph;
+    if (memory == SARBP_MEMORY_HOST) {
+        SARBP_TRY_CUDA(cudaMemcpyAsync(p->d_ph, ph, static_cast<size_t>(np) * p->K * 8, cudaMemcpyHostToDevice, s));
+        src = p->d_ph;
+    }
+    SARBP_TRY_CUDA(launch_rc_prep(p->precision, src, p->d_fac, p->d_fft, p->K, p->nfft, np, s));
+    const cufftResult r0 = cufftSetStream(p->fft, s);
+    if (r0 != CUFFT_SUCCESS) return from_cufft(r0);
+    const cufftResult r1 =
+        p->precision == SARBP_PRECISION_FP64
+            ? cufftExecZ2Z(p->fft, static_cast<cufftDoubleComplex *>(p->d_fft),
+                           static_cast<cufftDoubleComplex *>(p->d_fft), CUFFT_INVERSE)
+            : cufftExecC2C(p->fft, static_cast<cufftComplex *>(p->d_fft), static_cast<cufftComplex *>(p->d_fft),
+                           CUFFT_INVERSE);
+    if (r1 != CUFFT_SUCCESS) return from_cufft(r1);
+    SARBP_TRY_CUDA(launch_rc_pairs(p->precision, p->d_fft, p->d_pairs, p->nfft, np, p->row_stride, p->guard, s));
+    p->np_ready = np;
+    if (memory == SARBP_MEMORY_HOST) SARBP_TRY_CUDA(cudaStreamSynchronize(s));
+    return SARBP_OK;
+}
+
+int backproject_impl(sarbp_plan *p, const sarbp_geometry *geo, void *image, int image_memory, int flags,
+                     cudaStream_t s) {
+    if (!geo || !image || !geo->ant_x || !geo->ant_y || !geo->ant_z || !geo->slant_range || !geo->start_freq)
+        return SARBP_ERR_NULL_POINTER;
+    if (geo->num_pulses < 1 || geo->num_pulses > p->np_ready) return SARBP_ERR_INVALID_ARGUMENT;
+    if ((geo->memory != SARBP_MEMORY_HOST && geo->memory != SARBP_MEMORY_DEVICE) ||
+        (image_memory != SARBP_MEMORY_HOST && image_memory != SARBP_MEMORY_DEVICE) ||
+        (flags & ~(SARBP_ACCUMULATE | SARBP_CHECKED)))
+        return SARBP_ERR_INVALID_ARGUMENT;
+    const int np = geo->num_pulses;
+    const double *ax = geo->ant_x, *ay = geo->ant_y, *az = geo->ant_z, *r0 = geo->slant_range,
+                 *f0 = geo->start_freq;
+    if (geo->memory == SARBP_MEMORY_HOST) {
+        const int st = check_geometry_host(geo);
+        if (st != SARBP_OK) return st;
+        const double *src[5] = {ax, ay, az, r0, f0};
+        for (int i = 0; i < 5; ++i)
+            SARBP_TRY_CUDA(cudaMemcpyAsync(p->d_geo + static_cast<size_t>(i) * p->np_cap, src[i],
+                                           sizeof(double) * np, cudaMemcpyHostToDevice, s));
+        ax = p->d_geo;
+        ay = p->d_geo + p->np_cap;
+        az = p->d_geo + 2 * p->np_cap;
+        r0 = p->d_geo + 3 * p->np_cap;
+        f0 = p->d_geo + 4 * p->np_cap;
+    }
+    const sarbp_grid &g = p->desc.grid;
+    const size_t img_bytes = static_cast<size_t>(g.nx) * g.ny * g.nz * cplx_bytes(p);
+    void *dimg = image;
+    if (image_memory == SARBP_MEMORY_HOST) {
+        dimg = p->d_img;
+        if (flags & SARBP_ACCUMULATE)
+            SARBP_TRY_CUDA(cudaMemcpyAsync(dimg, image, img_bytes, cudaMemcpyHostToDevice, s));
+    }
+
+    BpLaunch L{};
+    L.pairs = p->d_pairs;
+    L.row_stride = p->row_stride;
+    L.guard = p->guard;
+    L.ax = ax;
+    L.ay = ay;
+    L.az = az;
+    L.r0 = r0;
+    L.f0 = f0;
+    L.np = np;
+    L.nfft = p->nfft;
+    L.lambda = p->lambda;
+    L.half_nfft = 0.5 * p->nfft;
+    L.nx = g.nx;
+    L.ny = g.ny;
+    L.nz = g.nz;
+    L.left = p->left;
+    L.bottom = p->bottom;
+    L.zlow = p->zlow;
+    L.dx = p->dx;
+    L.dy = p->dy;
+    L.dz = p->dz;
+    L.W = p->W;
+    L.wsize = p->wsize;
+    L.near_hd16 = p->near_hd16;
+    L.near_coef = p->near_coef;
+    L.img = dimg;
+    L.accumulate = (flags & SARBP_ACCUMULATE) ? 1 : 0;
+    L.vec_store = ((reinterpret_cast<uintptr_t>(dimg) & 15u) == 0 && (g.ny % 2) == 0) ? 1 : 0;
+    L.err = p->d_err;
+    cudaError_t e;
+    if (p->precision == SARBP_PRECISION_FP64)
+        e = launch_bp_fp64(L, p->tile, p->smem, s);
+    else
+        e = launch_bp_mixed(L, p->tile, (flags & SARBP_CHECKED) != 0, p->smem, s);
+    SARBP_TRY_CUDA(e);
+    if (image_memory == SARBP_MEMORY_HOST) {
+        SARBP_TRY_CUDA(cudaMemcpyAsync(image, dimg, img_bytes, cudaMemcpyDeviceToHost, s));
+        return read_errors(p, s);
+    }
+    if (geo->memory == SARBP_MEMORY_HOST) SARBP_TRY_CUDA(cudaStreamSynchronize(s));
+    return SARBP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sarbp_abi_version(void) { return SARBP_ABI_VERSION; }
+
+const char *sarbp_status_string(int status) {
+    switch (status) {
+        case SARBP_OK: return "ok";
+        case SARBP_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case SARBP_ERR_NULL_POINTER: return "null pointer";
+        case SARBP_ERR_UNSUPPORTED: return "unsupported configuration";
+        case SARBP_ERR_OUT_OF_MEMORY: return "out of memory";
+        case SARBP_ERR_CUDA: return "CUDA runtime error";
+        case SARBP_ERR_CUFFT: return "cuFFT error";
+        case SARBP_ERR_NOT_FINITE: return "non-finite geometry";
+        case SARBP_ERR_KERNEL_TIMEOUT: return "device wait timed out";
+        case SARBP_ERR_KERNEL_BOUNDS: return "kernel index out of range (clamped)";
+        case SARBP_ERR_NO_DEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+int sarbp_plan_create(const sarbp_plan_desc *desc, sarbp_plan **out) {
+    if (!out) return SARBP_ERR_NULL_POINTER;
+    *out = nullptr;
+    int st = validate_desc(desc);
+    if (st != SARBP_OK) return st;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return SARBP_ERR_NO_DEVICE;
+    }
+    int dev = desc->device;
+    if (dev < 0) SARBP_TRY_CUDA(cudaGetDevice(&dev));
+    if (dev >= ndev) return SARBP_ERR_INVALID_ARGUMENT;
+    DeviceGuard guard(dev);
+    SARBP_TRY_CUDA(guard.status);
+
+    sarbp_plan *p = new (std::nothrow) sarbp_plan();
+    if (!p) return SARBP_ERR_OUT_OF_MEMORY;
+    p->desc = *desc;
+    p->device = dev;
+    p->K = desc->num_range_samples;
+    p->np_cap = desc->num_pulses;
+    p->nfft = desc->nfft;
+    p->precision = desc->precision;
+    p->lambda = static_cast<double>(desc->nfft) / desc->max_wr;
+    const sarbp_grid &g = desc->grid;
+    axis(g.nx, g.x0, g.wx, &p->left, &p->dx);
+    axis(g.ny, g.y0, g.wy, &p->bottom, &p->dy);
+    axis(g.nz, g.z0, g.wz, &p->zlow, &p->dz);
+    st = choose_tile(p);
+    if (st != SARBP_OK) {
+        delete p;
+        return st;
+    }
+    {
+        const double hx = 0.5 * 8.0 * p->tile.mx * p->dx, hy = 0.5 * 64.0 * p->dy;
+        const double hd = std::sqrt(hx * hx + hy * hy);
+        // far-field remainder error <= 0.625 hd^4 / Rc^3 metres; keep k times
+        // it under 1e-7 revolutions, else the pulse takes the exact path
+        p->near_hd16 = 16.0 * hd;
+        p->near_coef = 0.625 * hd * hd * hd * hd / 1.0e-7;
+    }
+    p->guard = p->wsize + 2;
+    p->row_stride = static_cast<long long>(p->nfft) + 2LL * p->guard;
+    const size_t cb = cplx_bytes(p);
+    const size_t entry = p->precision == SARBP_PRECISION_FP64 ? 32 : 16;
+    const size_t npix = static_cast<size_t>(g.nx) * g.ny * g.nz;
+    const size_t np = static_cast<size_t>(p->np_cap);
+    if ((st = alloc(p, &p->d_ph, np * p->K * 8)) ||
+        (st = alloc(p, reinterpret_cast<void **>(&p->d_geo), 5 * np * sizeof(double))) ||
+        (st = alloc(p, &p->d_fft, np * p->nfft * cb)) ||
+        (st = alloc(p, &p->d_pairs, np * static_cast<size_t>(p->row_stride) * entry)) ||
+        (st = alloc(p, &p->d_fac, static_cast<size_t>(p->K) * cb)) || (st = alloc(p, &p->d_img, npix * cb)) ||
+        (st = alloc(p, reinterpret_cast<void **>(&p->d_err), sizeof(unsigned)))) {
+        release(p);
+        return st;
+    }
+    if (cudaMemset(p->d_pairs, 0, np * static_cast<size_t>(p->row_stride) * entry) != cudaSuccess ||
+        cudaMemset(p->d_fft, 0, np * p->nfft * cb) != cudaSuccess ||
+        cudaMemset(p->d_err, 0, sizeof(unsigned)) != cudaSuccess) {
+        cudaGetLastError();
+        release(p);
+        return SARBP_ERR_CUDA;
+    }
+    // fac[k] = w_k / nfft * exp(+j 2 pi ((k s) mod nfft) / nfft), s = (nfft+1)/2
+    {
+        const int K = p->K, N = p->nfft;
+        const long long s = (N + 1) / 2;
+        std::vector<double> fac(2 * static_cast<size_t>(K));
+        for (int k = 0; k < K; ++k) {
+            double w = 1.0;
+            if (desc->window == SARBP_WINDOW_HAMMING && K > 1)
+                w = 0.54 - 0.46 * std::cos(2.0 * M_PI * static_cast<double>(k) / static_cast<double>(K - 1));
+            const long long m = (static_cast<long long>(k) * s) % N;
+            const double ang = 2.0 * M_PI * static_cast<double>(m) / static_cast<double>(N);
+            fac[2 * k] = w / N * std::cos(ang);
+            fac[2 * k + 1] = w / N * std::sin(ang);
+        }
+        cudaError_t e;
+        if (p->precision == SARBP_PRECISION_FP64) {
+            e = cudaMemcpy(p->d_fac, fac.data(), fac.size() * sizeof(double), cudaMemcpyHostToDevice);
+        } else {
+            std::vector<float> f32(fac.begin(), fac.end());
+            e = cudaMemcpy(p->d_fac, f32.data(), f32.size() * sizeof(float), cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            release(p);
+            return from_cuda(e);
+        }
+    }
+    const cufftResult r = cufftPlan1d(&p->fft, p->nfft, p->precision == SARBP_PRECISION_FP64 ? CUFFT_Z2Z : CUFFT_C2C,
+                                      p->np_cap);
+    if (r != CUFFT_SUCCESS) {
+        release(p);
+        return from_cufft(r);
+    }
+    p->fft_ok = true;
+    size_t ws = 0;
+    if (cufftGetSize(p->fft, &ws) == CUFFT_SUCCESS) p->bytes += ws;
+    *out = p;
+    return SARBP_OK;
+}
+
+int sarbp_plan_destroy(sarbp_plan *plan) {
+    if (!plan) return SARBP_ERR_NULL_POINTER;
+    DeviceGuard guard(plan->device);
+    release(plan);
+    return SARBP_OK;
+}
+
+int sarbp_plan_workspace_bytes(const sarbp_plan *plan, size_t *bytes) {
+    if (!plan || !bytes) return SARBP_ERR_NULL_POINTER;
+    *bytes = plan->bytes;
+    return SARBP_OK;
+}
+
+int sarbp_range_compress(sarbp_plan *plan, const void *phase_history, int num_pulses, int memory, void *stream) {
+    if (!plan) return SARBP_ERR_NULL_POINTER;
+    DeviceGuard guard(plan->device);
+    SARBP_TRY_CUDA(guard.status);
+    return range_compress_impl(plan, phase_history, num_pulses, memory, static_cast<cudaStream_t>(stream));
+}
+
+int sarbp_get_range_profiles(sarbp_plan *plan, void *out, int memory, void *stream) {
+    if (!plan || !out) return SARBP_ERR_NULL_POINTER;
+    if (memory != SARBP_MEMORY_HOST && memory != SARBP_MEMORY_DEVICE) return SARBP_ERR_INVALID_ARGUMENT;
+    if (plan->np_ready < 1) return SARBP_ERR_INVALID_ARGUMENT;
+    DeviceGuard guard(plan->device);
+    SARBP_TRY_CUDA(guard.status);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t bytes = static_cast<size_t>(plan->np_ready) * plan->nfft * cplx_bytes(plan);
+    SARBP_TRY_CUDA(cudaMemcpyAsync(out, plan->d_fft, bytes,
+                                   memory == SARBP_MEMORY_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                   s));
+    if (memory == SARBP_MEMORY_HOST) SARBP_TRY_CUDA(cudaStreamSynchronize(s));
+    return SARBP_OK;
+}
+
+int sarbp_backproject(sarbp_plan *plan, const sarbp_geometry *geometry, void *image, int image_memory, int flags,
+                      void *stream) {
+    if (!plan) return SARBP_ERR_NULL_POINTER;
+    DeviceGuard guard(plan->device);
+    SARBP_TRY_CUDA(guard.status);
+    return backproject_impl(plan, geometry, image, image_memory, flags, static_cast<cudaStream_t>(stream));
+}
+
+int sarbp_focus(sarbp_plan *plan, const sarbp_aperture *ap, void *image, int image_memory, void *stream) {
+    if (!plan || !ap) return SARBP_ERR_NULL_POINTER;
+    DeviceGuard guard(plan->device);
+    SARBP_TRY_CUDA(guard.status);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int st = range_compress_impl(plan, ap->phase_history, ap->geometry.num_pulses, ap->phase_history_memory, s);
+    if (st != SARBP_OK) return st;
+    return backproject_impl(plan, &ap->geometry, image, image_memory, 0, s);
+}
+
+int sarbp_focus_image(const sarbp_plan_desc *desc, const sarbp_aperture *ap, void *image, int image_memory) {
+    if (!desc || !ap) return SARBP_ERR_NULL_POINTER;
+    sarbp_plan *plan = nullptr;
+    int st = sarbp_plan_create(desc, &plan);
+    if (st != SARBP_OK) return st;
+    st = sarbp_focus(plan, ap, image, image_memory, nullptr);
+    if (st == SARBP_OK) st = sarbp_plan_check(plan, nullptr);
+    sarbp_plan_destroy(plan);
+    return st;
+}
+
+int sarbp_plan_check(sarbp_plan *plan, void *stream) {
+    if (!plan) return SARBP_ERR_NULL_POINTER;
+    DeviceGuard guard(plan->device);
+    SARBP_TRY_CUDA(guard.status);
+    return read_errors(plan, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

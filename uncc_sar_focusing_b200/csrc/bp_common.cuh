@@ -1,0 +1,139 @@
+// bp_common.cuh -- shared device helpers of the sm_100a backprojection kernels.
+//
+// * mbarrier + cp.async.bulk (the non-tensor TMA copy, no multicast) used to
+//   stage each pulse's range-bin window of a pixel tile into shared memory;
+// * bounded waits: every wait gives up after a fixed wall time, sets an error
+//   bit and lets the kernel return instead of hanging;
+// * the per-(tile, pulse) geometry record computed in FP64 once per tile and
+//   pulse and read by every thread of the tile.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sarbp {
+
+// Device error bits (plan->d_err)
+enum : unsigned {
+    ERRBIT_NOT_FINITE = 1u,
+    ERRBIT_TIMEOUT = 2u,
+    ERRBIT_BOUNDS = 4u,
+};
+
+// speed of light, include/uncc_sar_focusing.hpp:34
+constexpr double kClight = 299792458.0;
+
+// Wall-clock limit of a bounded wait (ns).
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long global_timer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for phase `parity` of the barrier; false (and an error bit) after the
+// wall-clock limit.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, unsigned *err) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_timer_ns();
+    for (unsigned it = 1;; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 255u) == 0u && global_timer_ns() - t0 > kWaitLimitNs) {
+            atomicOr(err, ERRBIT_TIMEOUT);
+            return false;
+        }
+    }
+}
+
+// Plain (non-multicast) bulk copy global -> this CTA's shared memory,
+// completing transaction bytes on `bar`.  dst, src and bytes are multiples
+// of 16 (the callers copy whole 16- or 32-byte entries from 256-byte aligned
+// allocations).
+__device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ double frac_rev(double x) { return x - rint(x); }
+
+// Flags of a PulseGeo record
+enum : int {
+    PG_ACTIVE = 1,  // the tile's window meets the valid range bins
+    PG_GATE = 2,    // some pixels may fall outside (0, nfft-1): test each
+    PG_NEAR = 4,    // tile too large for the far-field expansion: exact path
+};
+
+// Geometry of one pulse relative to one pixel tile (mixed-precision kernel).
+//
+// With the tile centre c on the pixel grid, pixel offset d = (i*dx, j*dy, 0)
+// (integers i, j), u = (a - c)/|a - c|, Rc = |a - c|, t = u.d and
+// e = |d|^2 - t^2, the differential range is exactly
+//     dR = (Rc - R0) - t + g,   g = e / ((Rc - t) + sqrt((Rc - t)^2 + e))
+// and g = e (h + t hr) (1 + O((|d|/Rc)^2)) with h = 1/(2Rc), hr = 1/(2Rc^2).
+// Phase (revolutions) k dR, k = 2 f0 / c; range bin lambda dR + nfft/2,
+// lambda = nfft / max_wr.  The linear terms are reduced modulo one
+// revolution in FP64 so the FP32 remainder stays small.
+struct __align__(16) PulseGeo {
+    double A;      // frac(k (Rc - R0))
+    double alpha;  // frac(-k ux dx): revolutions per x step
+    double beta;   // frac(-k uy dy): revolutions per y step
+    double B0;     // tile-centre bin relative to the window start
+    double gam;    // -lambda ux dx: bins per x step
+    double eta;    // -lambda uy dy: bins per y step
+    float a8;      // frac(8 alpha): a thread's rows are 8 apart
+    float b1;      // beta
+    float g8;      // 8 gam
+    float e1;      // eta
+    float tx, ty;  // ux dx, uy dy (metres per step, for t)
+    float h, hr;   // 1/(2 Rc), 1/(2 Rc^2)
+    float kappa;   // k (revolutions per metre)
+    float rc;      // Rc (exact path)
+    float lo, hi;  // valid iff lo < B_rel < hi, i.e. 0 < bin < nfft-1
+    int ws;        // window start bin (may be negative: guard band)
+    int flags;     // PG_*
+    int pad0, pad1;
+};
+static_assert(sizeof(PulseGeo) % 16 == 0, "PulseGeo must keep 16-byte alignment");
+
+// Geometry of one pulse for the FP64 kernel (per-pixel exact computation).
+struct __align__(16) PulseGeo64 {
+    double ax, ay, az;  // antenna position
+    double r0;          // slant range to scene centre
+    double k;           // 2 f0 / c
+    int ws;             // window start bin
+    int flags;          // PG_ACTIVE
+};
+static_assert(sizeof(PulseGeo64) % 16 == 0, "PulseGeo64 must keep 16-byte alignment");
+
+}  // namespace sarbp

@@ -1,0 +1,76 @@
+// sarbp_internal.h -- plan state and kernel launchers behind include/sarbp.h.
+#pragma once
+
+#include <cstddef>
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include "../../include/sarbp.h"
+
+namespace sarbp {
+
+// Launch parameters of the forward backprojection kernels.
+struct BpLaunch {
+    const void *pairs;      // float4 (MIXED) / double4 (FP64) pair entries
+    long long row_stride;   // entries per pulse row
+    int guard;              // zero entries before bin 0 of each row
+    const double *ax, *ay, *az, *r0, *f0;
+    int np, nfft;
+    double lambda;          // nfft / max_wr (bins per metre)
+    double half_nfft;       // nfft / 2
+    int nx, ny, nz;
+    double left, bottom, zlow;  // coordinates of pixel (0, 0, 0)
+    double dx, dy, dz;
+    int W, wsize;           // window half-width and size (entries)
+    double near_hd16;       // 16 * tile half-diagonal (m)
+    double near_coef;       // 0.625 * hd^4 / tolerance (revolutions)
+    void *img;              // complex64 / complex128 [nz][nx][ny]
+    int accumulate;
+    int vec_store;          // 16-byte aligned image and even ny
+    unsigned *err;
+};
+
+// Tile shape of the forward kernels (see bp_mixed.cu).
+struct TileConfig {
+    int mx;   // rows per thread; tile = (8*mx) x 64 pixels, 256 threads
+    int pb;   // pulses per pipeline stage
+};
+
+cudaError_t launch_bp_mixed(const BpLaunch &L, const TileConfig &tc, bool checked, size_t smem,
+                            cudaStream_t s);
+cudaError_t launch_bp_fp64(const BpLaunch &L, const TileConfig &tc, size_t smem, cudaStream_t s);
+size_t bp_mixed_smem_bytes(const TileConfig &tc, int wsize);
+size_t bp_fp64_smem_bytes(const TileConfig &tc, int wsize);
+
+// Range compression kernels (range_compress.cu)
+cudaError_t launch_rc_prep(int precision, const void *ph, const void *fac, void *fft_buf, int K, int nfft, int np,
+                           cudaStream_t s);
+cudaError_t launch_rc_pairs(int precision, const void *fft_buf, void *pairs, int nfft, int np, long long row_stride,
+                            int guard, cudaStream_t s);
+
+}  // namespace sarbp
+
+struct sarbp_plan {
+    sarbp_plan_desc desc;
+    int device;
+    int K, np_cap, nfft, precision;
+    double lambda;
+    int W, wsize, guard;
+    long long row_stride;
+    sarbp::TileConfig tile;
+    size_t smem;
+    double near_hd16, near_coef;
+    double dx, dy, dz, left, bottom, zlow;
+
+    void *d_ph;       // complex64 [np][K] staging for host phase histories
+    double *d_geo;    // 5 x np staging for host geometry
+    void *d_fft;      // complex64/128 [np][nfft]
+    void *d_pairs;    // pair entries [np][row_stride]
+    void *d_fac;      // per-sample window * scale * shift twiddle [K]
+    void *d_img;      // image staging for host outputs
+    unsigned *d_err;  // device error bits
+    size_t bytes;     // device bytes held
+    cufftHandle fft;
+    bool fft_ok;
+    int np_ready;     // pulses in the current range profiles
+};

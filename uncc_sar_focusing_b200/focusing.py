@@ -1,0 +1,190 @@
+"""Python front-end of the C ABI (include/sarbp.h).
+
+`Plan` owns a sarbp_plan: device buffers and the FFT plan for one aperture
+shape and image grid.  Arrays may be numpy arrays (host memory: the call
+copies in and out and synchronises) or CUDA torch tensors (device memory:
+the call is enqueued on torch's current stream and returns immediately).
+Torch is only the device-memory and stream provider here; all computation
+happens in libsarbp.so.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _native as N
+from .scenes import CLIGHT, Grid, Scene
+
+_PRECISION = {"mixed": N.PRECISION_MIXED, "fp64": N.PRECISION_FP64}
+_WINDOW = {None: N.WINDOW_NONE, "none": N.WINDOW_NONE, "hamming": N.WINDOW_HAMMING}
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _ptr(x, dtype, count: Optional[int] = None):
+    """(pointer, memory kind, keep-alive) of a numpy array or CUDA tensor."""
+    if _is_torch(x):
+        import torch
+
+        want = {np.float64: torch.float64, np.complex64: torch.complex64, np.complex128: torch.complex128}[dtype]
+        if not x.is_cuda:
+            raise ValueError("torch tensors passed to the engine must live on a CUDA device")
+        if x.dtype != want or not x.is_contiguous():
+            raise ValueError(f"expected a contiguous {want} tensor, got {x.dtype}")
+        if count is not None and x.numel() < count:
+            raise ValueError(f"tensor has {x.numel()} elements, need {count}")
+        return ctypes.c_void_p(x.data_ptr()), N.MEMORY_DEVICE, x
+    a = np.ascontiguousarray(x, dtype=dtype)
+    if count is not None and a.size < count:
+        raise ValueError(f"array has {a.size} elements, need {count}")
+    return ctypes.c_void_p(a.ctypes.data), N.MEMORY_HOST, a
+
+
+def _stream(*arrays):
+    if any(_is_torch(a) for a in arrays):
+        import torch
+
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return ctypes.c_void_p(0)
+
+
+class Plan:
+    """Device state for focusing apertures of K samples x <= num_pulses
+    pulses onto one grid (sarbp_plan_create)."""
+
+    def __init__(self, num_range_samples: int, num_pulses: int, nfft: int, max_wr: float, grid: Grid,
+                 precision: str = "mixed", window: Optional[str] = "hamming", device: int = -1):
+        self.K = int(num_range_samples)
+        self.np_cap = int(num_pulses)
+        self.nfft = int(nfft)
+        self.grid = grid
+        self.precision = precision
+        self.image_dtype = np.complex128 if precision == "fp64" else np.complex64
+        d = N.PlanDesc()
+        d.num_range_samples = self.K
+        d.num_pulses = self.np_cap
+        d.nfft = self.nfft
+        d.max_wr = float(max_wr)
+        d.grid = N.Grid(grid.nx, grid.ny, grid.nz, grid.x0, grid.y0, grid.z0, grid.wx, grid.wy, grid.wz)
+        d.precision = _PRECISION[precision]
+        d.window = _WINDOW[window]
+        d.device = int(device)
+        self._desc = d
+        h = ctypes.c_void_p()
+        N.check(N.lib().sarbp_plan_create(ctypes.byref(d), ctypes.byref(h)), "sarbp_plan_create")
+        self._h = h
+        self.num_pulses_ready = 0
+
+    @classmethod
+    def for_scene(cls, scene: Scene, precision: str = "mixed", device: int = -1) -> "Plan":
+        return cls(scene.num_range_samples, scene.num_pulses, scene.nfft, scene.max_wr, scene.grid,
+                   precision=precision, window=scene.window, device=device)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            N.lib().sarbp_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def workspace_bytes(self) -> int:
+        v = ctypes.c_size_t()
+        N.check(N.lib().sarbp_plan_workspace_bytes(self._h, ctypes.byref(v)), "sarbp_plan_workspace_bytes")
+        return int(v.value)
+
+    def image_shape(self):
+        g = self.grid
+        return (g.nz, g.nx, g.ny)
+
+    def new_image(self, device: Optional[str] = None):
+        if device is None:
+            return np.zeros(self.image_shape(), dtype=self.image_dtype)
+        import torch
+
+        dt = torch.complex128 if self.precision == "fp64" else torch.complex64
+        return torch.zeros(self.image_shape(), dtype=dt, device=device)
+
+    # -- entry points -------------------------------------------------------
+    def range_compress(self, phase_history) -> None:
+        n = int(phase_history.shape[0])
+        p, mem, keep = _ptr(phase_history, np.complex64, n * self.K)
+        st = N.lib().sarbp_range_compress(self._h, p, n, mem, _stream(phase_history))
+        N.check(st, "sarbp_range_compress")
+        self.num_pulses_ready = n
+
+    def range_profiles(self, out=None):
+        n = self.num_pulses_ready
+        dt = np.complex128 if self.precision == "fp64" else np.complex64
+        if out is None:
+            out = np.empty((n, self.nfft), dtype=dt)
+        p, mem, keep = _ptr(out, dt, n * self.nfft)
+        N.check(N.lib().sarbp_get_range_profiles(self._h, p, mem, _stream(out)), "sarbp_get_range_profiles")
+        return out
+
+    def _geometry(self, ant_x, ant_y, ant_z, slant_range, start_freq):
+        n = int(ant_x.shape[0])
+        ptrs = [_ptr(v, np.float64, n) for v in (ant_x, ant_y, ant_z, slant_range, start_freq)]
+        mems = {m for _, m, _ in ptrs}
+        if len(mems) != 1:
+            raise ValueError("geometry arrays must all be host arrays or all CUDA tensors")
+        g = N.Geometry(ptrs[0][0], ptrs[1][0], ptrs[2][0], ptrs[3][0], ptrs[4][0], n, mems.pop())
+        return g, [k for _, _, k in ptrs]
+
+    def backproject(self, ant_x, ant_y, ant_z, slant_range, start_freq, out=None, accumulate: bool = False,
+                    checked: bool = False):
+        geo, keep = self._geometry(ant_x, ant_y, ant_z, slant_range, start_freq)
+        if out is None:
+            out = self.new_image(None if geo.memory == N.MEMORY_HOST else "cuda")
+        ip, imem, ikeep = _ptr(out, self.image_dtype, int(np.prod(self.image_shape())))
+        flags = (N.ACCUMULATE if accumulate else 0) | (N.CHECKED if checked else 0)
+        st = N.lib().sarbp_backproject(self._h, ctypes.byref(geo), ip, imem, flags,
+                                       _stream(out, ant_x))
+        N.check(st, "sarbp_backproject")
+        if imem == N.MEMORY_HOST and ikeep is not out:
+            np.copyto(out, ikeep.reshape(out.shape))
+        return out
+
+    def focus(self, phase_history, ant_x, ant_y, ant_z, slant_range, start_freq, out=None):
+        geo, keep = self._geometry(ant_x, ant_y, ant_z, slant_range, start_freq)
+        if int(phase_history.shape[0]) != geo.num_pulses:
+            raise ValueError("phase history and geometry disagree on the pulse count")
+        pp, pmem, pkeep = _ptr(phase_history, np.complex64, geo.num_pulses * self.K)
+        ap = N.Aperture(pp, pmem, geo)
+        if out is None:
+            out = self.new_image(None if pmem == N.MEMORY_HOST and geo.memory == N.MEMORY_HOST else "cuda")
+        ip, imem, ikeep = _ptr(out, self.image_dtype, int(np.prod(self.image_shape())))
+        st = N.lib().sarbp_focus(self._h, ctypes.byref(ap), ip, imem, _stream(out, phase_history, ant_x))
+        N.check(st, "sarbp_focus")
+        self.num_pulses_ready = geo.num_pulses
+        if imem == N.MEMORY_HOST and ikeep is not out:
+            np.copyto(out, ikeep.reshape(out.shape))
+        return out
+
+    def check(self) -> None:
+        """Synchronise and raise if a kernel recorded an error."""
+        import torch
+
+        s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream) if torch.cuda.is_available() else None
+        N.check(N.lib().sarbp_plan_check(self._h, s), "sarbp_plan_check")
+
+
+def focus_scene(scene: Scene, precision: str = "mixed") -> np.ndarray:
+    """Focus a scene through host buffers (sarbp_focus on host memory)."""
+    with Plan.for_scene(scene, precision) as plan:
+        return plan.focus(scene.phase_history, scene.ant_x, scene.ant_y, scene.ant_z, scene.slant_range,
+                          scene.start_freq)
