@@ -57,6 +57,9 @@ def parse_args():
     ap.add_argument("--config", choices=["large", "point_targets"], default="large")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
+    ap.add_argument("--profile", action="store_true",
+                    help="one warm-up and one focus step of the workload, nothing else (for ncu captures)")
+    ap.add_argument("--pulses", type=int, default=0, help="use only the first N pulses (profiling)")
     return ap.parse_args()
 
 
@@ -400,10 +403,42 @@ def gpu_arm(args):
     return 0
 
 
+def profile_arm(args):
+    """A single focus of the workload after one warm-up, with the scene
+    synthesis temporaries released first so that a profiler's per-pass memory
+    save/restore only covers the plan and the inputs."""
+    import numpy as np
+    import torch
+
+    from uncc_sar_focusing_b200 import focusing
+
+    torch.cuda.set_device(0)
+    sc, _ = make_scene(args.config, 0, 1, "cuda")
+    if args.pulses:
+        n = args.pulses
+        sc.phase_history = sc.phase_history[:n]
+        sc.ant_x, sc.ant_y, sc.ant_z = sc.ant_x[:n], sc.ant_y[:n], sc.ant_z[:n]
+        sc.slant_range, sc.start_freq = sc.slant_range[:n], sc.start_freq[:n]
+    torch.cuda.empty_cache()
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    ph = d(sc.phase_history)
+    geo = [d(v) for v in (sc.ant_x, sc.ant_y, sc.ant_z, sc.slant_range, sc.start_freq)]
+    with focusing.Plan.for_scene(sc, "mixed", device=0) as plan:
+        img = plan.new_image("cuda")
+        for _ in range(2):
+            plan.focus(ph, *geo, out=img)
+        torch.cuda.synchronize()
+        plan.check()
+    print(json.dumps({"profile": args.config, "pulses": sc.num_pulses, "pixel_pulses": sc.pixel_pulses}))
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.profile:
+        return profile_arm(args)
     return gpu_arm(args)
 
 

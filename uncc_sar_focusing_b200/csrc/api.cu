@@ -103,36 +103,37 @@ void window_for(const sarbp_plan *p, int mx, int *W, int *wsize) {
 // Largest stage depth whose shared memory fits 2 CTAs per SM (mixed) or one
 // (FP64); environment SARBP_TILE="mx,pb" overrides (tuning runs).
 int choose_tile(sarbp_plan *p) {
-    static const int cand_mixed[][2] = {{4, 8}, {4, 4}, {2, 8}, {2, 4}, {1, 8}};
-    static const int cand_fp64[][2] = {{4, 4}, {2, 4}, {1, 8}};
+    // (mx, pb) candidates, best first; the first pass keeps two CTAs per SM
+    // for the mixed kernel, the second accepts one CTA per SM (coarse grids
+    // whose range-bin windows are wide)
+    static const int cand[][2] = {{4, 8}, {4, 4}, {2, 8}, {2, 4}, {1, 8}, {1, 4}, {2, 2}, {1, 2}, {1, 1}};
+    const int ncand = static_cast<int>(sizeof(cand) / sizeof(cand[0]));
     const bool fp64 = p->precision == SARBP_PRECISION_FP64;
-    const size_t limit = fp64 ? 220u * 1024u : 110u * 1024u;
     int forced_mx = 0, forced_pb = 0;
     if (const char *env = std::getenv("SARBP_TILE")) {
         if (std::sscanf(env, "%d,%d", &forced_mx, &forced_pb) != 2) forced_mx = forced_pb = 0;
     }
-    const int n = fp64 ? 3 : 5;
-    for (int i = -1; i < n; ++i) {
-        int mx, pb;
-        if (i < 0) {
-            if (!forced_mx) continue;
-            mx = forced_mx;
-            pb = forced_pb;
-        } else {
-            mx = fp64 ? cand_fp64[i][0] : cand_mixed[i][0];
-            pb = fp64 ? cand_fp64[i][1] : cand_mixed[i][1];
+    const size_t limits[2] = {fp64 ? 220u * 1024u : 110u * 1024u, 227u * 1024u};
+    for (int pass = -1; pass < 2; ++pass) {
+        for (int i = 0; i < ncand; ++i) {
+            int mx = cand[i][0], pb = cand[i][1];
+            if (pass < 0) {
+                if (!forced_mx || i > 0) break;
+                mx = forced_mx;
+                pb = forced_pb;
+            }
+            int W, wsize;
+            window_for(p, mx, &W, &wsize);
+            if (wsize > (1 << 16)) continue;
+            TileConfig tc{mx, pb};
+            const size_t smem = fp64 ? bp_fp64_smem_bytes(tc, wsize) : bp_mixed_smem_bytes(tc, wsize);
+            if (smem > limits[pass < 0 ? 1 : pass]) continue;
+            p->tile = tc;
+            p->W = W;
+            p->wsize = wsize;
+            p->smem = smem;
+            return SARBP_OK;
         }
-        int W, wsize;
-        window_for(p, mx, &W, &wsize);
-        if (wsize > (1 << 16)) continue;
-        TileConfig tc{mx, pb};
-        const size_t smem = fp64 ? bp_fp64_smem_bytes(tc, wsize) : bp_mixed_smem_bytes(tc, wsize);
-        if (smem > (i < 0 ? 227u * 1024u : limit)) continue;
-        p->tile = tc;
-        p->W = W;
-        p->wsize = wsize;
-        p->smem = smem;
-        return SARBP_OK;
     }
     return SARBP_ERR_UNSUPPORTED;
 }

@@ -48,6 +48,10 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t byt
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -101,30 +105,22 @@ enum : int {
 // e = |d|^2 - t^2, the differential range is exactly
 //     dR = (Rc - R0) - t + g,   g = e / ((Rc - t) + sqrt((Rc - t)^2 + e))
 // and g = e (h + t hr) (1 + O((|d|/Rc)^2)) with h = 1/(2Rc), hr = 1/(2Rc^2).
-// Phase (revolutions) k dR, k = 2 f0 / c; range bin lambda dR + nfft/2,
-// lambda = nfft / max_wr.  The linear terms are reduced modulo one
-// revolution in FP64 so the FP32 remainder stays small.
+// Phase 2 pi k dR (k = 2 f0 / c), range bin lambda dR + nfft/2
+// (lambda = nfft / max_wr).  The per-tile and per-step phase terms are
+// reduced modulo one revolution in FP64, so what is left for FP32 is small.
+// Field groups are 16-byte aligned so a thread reads them with vector loads.
 struct __align__(16) PulseGeo {
-    double A;      // frac(k (Rc - R0))
-    double alpha;  // frac(-k ux dx): revolutions per x step
-    double beta;   // frac(-k uy dy): revolutions per y step
-    double B0;     // tile-centre bin relative to the window start
-    double gam;    // -lambda ux dx: bins per x step
-    double eta;    // -lambda uy dy: bins per y step
-    float a8;      // frac(8 alpha): a thread's rows are 8 apart
-    float b1;      // beta
-    float g8;      // 8 gam
-    float e1;      // eta
-    float tx, ty;  // ux dx, uy dy (metres per step, for t)
-    float h, hr;   // 1/(2 Rc), 1/(2 Rc^2)
-    float kappa;   // k (revolutions per metre)
-    float rc;      // Rc (exact path)
-    float lo, hi;  // valid iff lo < B_rel < hi, i.e. 0 < bin < nfft-1
-    int ws;        // window start bin (may be negative: guard band)
-    int flags;     // PG_*
+    double A, alpha;   // frac(k (Rc - R0)); frac(-k ux dx): revolutions per x step
+    double beta, B0;   // frac(-k uy dy); tile-centre bin relative to the window start
+    double gam, eta;   // -lambda ux dx, -lambda uy dy: bins per x / y step
+    float a8r, b1r, g8, e1;  // 2 pi frac(8 alpha), 2 pi beta (rad); 8 gam, eta (bins)
+    float tx, ty, h, hr;     // ux dx, uy dy (m); 1/(2 Rc), 1/(2 Rc^2)
+    float kr, rc, lo, hi;    // 2 pi k (rad/m); Rc; valid iff lo < B_rel < hi
+    int ws;                  // window start bin (may be negative: guard band)
+    int flags;               // PG_*
     int pad0, pad1;
 };
-static_assert(sizeof(PulseGeo) % 16 == 0, "PulseGeo must keep 16-byte alignment");
+static_assert(sizeof(PulseGeo) == 112, "PulseGeo layout");
 
 // Geometry of one pulse for the FP64 kernel (per-pixel exact computation).
 struct __align__(16) PulseGeo64 {

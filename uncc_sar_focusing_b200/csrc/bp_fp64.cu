@@ -42,26 +42,27 @@ __device__ __forceinline__ PulseGeo64 make_geo64(const BpLaunch &L, int p, doubl
     return g;
 }
 
+// As produce_slots in bp_mixed.cu: warp w handles pulse slots w, w + 8, ...
 template <int PB>
-__device__ __forceinline__ void produce_block64(const BpLaunch &L, int b, PulseGeo64 *geo_s, PairD *win_s,
-                                                uint32_t bar, int lane, double cx, double cy, double cz) {
-    const int p = b * PB + lane;
-    uint32_t bytes = 0;
-    const PairD *src = nullptr;
-    if (lane < PB) {
+__device__ __forceinline__ void produce_slots64(const BpLaunch &L, int b, PulseGeo64 *geo_s, uint32_t win_s,
+                                                uint32_t bar, int warp, int lane, double cx, double cy, double cz) {
+    if (lane != 0) return;
+    for (int q = warp; q < PB; q += kThreads / 32) {
+        const int p = b * PB + q;
         PulseGeo64 g;
         g.flags = 0;
         if (p < L.np) g = make_geo64(L, p, cx, cy, cz);
+        geo_s[q] = g;
         if (g.flags & PG_ACTIVE) {
-            bytes = static_cast<uint32_t>(L.wsize) * 32u;
-            src = static_cast<const PairD *>(L.pairs) + static_cast<long long>(p) * L.row_stride + L.guard + g.ws;
+            const uint32_t bytes = static_cast<uint32_t>(L.wsize) * 32u;
+            const PairD *src =
+                static_cast<const PairD *>(L.pairs) + static_cast<long long>(p) * L.row_stride + L.guard + g.ws;
+            mbar_arrive_expect_tx(bar, bytes);
+            bulk_copy_g2s(win_s + static_cast<uint32_t>(q) * bytes, src, bytes, bar);
+        } else {
+            mbar_arrive(bar);
         }
-        geo_s[lane] = g;
     }
-    const uint32_t total = __reduce_add_sync(0xffffffffu, bytes);
-    if (lane == 0) mbar_arrive_expect_tx(bar, total);
-    __syncwarp();
-    if (bytes) bulk_copy_g2s(smem_addr(win_s + lane * L.wsize), src, bytes, bar);
 }
 
 template <int MX, int PB>
@@ -93,23 +94,23 @@ __global__ void __launch_bounds__(kThreads, 1) bp_fp64_kernel(const BpLaunch L) 
 
     const uint32_t bar_base = smem_addr(&bars[0]);  // stage s barrier at bar_base + 8*s
     if (threadIdx.x == 0) {
-        mbar_init(bar_base, 1);
-        mbar_init(bar_base + 8, 1);
+        mbar_init(bar_base, PB);
+        mbar_init(bar_base + 8, PB);
         fence_mbar_init();
     }
     __syncthreads();
 
     const int nblocks = (L.np + PB - 1) / PB;
-    if (warp == 0 && nblocks > 0) produce_block64<PB>(L, 0, geo, win, bar_base, lane, cx, cy, cz);
+    if (nblocks > 0) produce_slots64<PB>(L, 0, geo, smem_addr(win), bar_base, warp, lane, cx, cy, cz);
     __syncthreads();
 
     int last_issued = 0;
     bool timed_out = false;
     for (int b = 0; b < nblocks; ++b) {
         const int s = b & 1;
-        if (warp == 0 && b + 1 < nblocks) {
-            produce_block64<PB>(L, b + 1, geo + (s ^ 1) * PB, win + (s ^ 1) * PB * wsize, bar_base + 8 * (s ^ 1), lane, cx, cy,
-                                cz);
+        if (b + 1 < nblocks) {
+            produce_slots64<PB>(L, b + 1, geo + (s ^ 1) * PB, smem_addr(win + (s ^ 1) * PB * wsize),
+                                bar_base + 8 * (s ^ 1), warp, lane, cx, cy, cz);
             last_issued = b + 1;
         }
         const bool ok = mbar_wait_bounded(bar_base + 8 * s, (b >> 1) & 1, L.err);
@@ -202,14 +203,21 @@ size_t bp_fp64_smem_bytes(const TileConfig &tc, int wsize) {
 cudaError_t launch_bp_fp64(const BpLaunch &L, const TileConfig &tc, size_t smem, cudaStream_t s) {
 #define SARBP_FP64_CASE(MX_, PB_) \
     if (tc.mx == MX_ && tc.pb == PB_) return launch64<MX_, PB_>(L, smem, s);
-    SARBP_FP64_CASE(4, 4)
-    SARBP_FP64_CASE(4, 8)
     SARBP_FP64_CASE(4, 16)
-    SARBP_FP64_CASE(2, 4)
-    SARBP_FP64_CASE(2, 8)
+    SARBP_FP64_CASE(4, 8)
+    SARBP_FP64_CASE(4, 4)
+    SARBP_FP64_CASE(4, 2)
+    SARBP_FP64_CASE(4, 1)
     SARBP_FP64_CASE(2, 16)
-    SARBP_FP64_CASE(1, 8)
+    SARBP_FP64_CASE(2, 8)
+    SARBP_FP64_CASE(2, 4)
+    SARBP_FP64_CASE(2, 2)
+    SARBP_FP64_CASE(2, 1)
     SARBP_FP64_CASE(1, 16)
+    SARBP_FP64_CASE(1, 8)
+    SARBP_FP64_CASE(1, 4)
+    SARBP_FP64_CASE(1, 2)
+    SARBP_FP64_CASE(1, 1)
 #undef SARBP_FP64_CASE
     return cudaErrorInvalidValue;
 }

@@ -10,20 +10,23 @@
 //     GPU kernel's roundf bracket, cuda_BackProjectionKernels.cuh:68-74).
 //
 // Design (one CTA = one pixel tile of (8*MX) x 64 pixels of one z-slice,
-// 256 threads, each thread MX rows x 2 adjacent columns):
-//  * per (tile, pulse), warp 0 computes the geometry record in FP64 (tile
-//    centre range, unit vector, phase and bin offsets reduced mod 1) and
-//    issues one cp.async.bulk copy of the pulse's range-bin window (the bins
-//    any pixel of the tile can touch, a conservative +-|tile half-diagonal|)
-//    into shared memory; two stages, PB pulses per stage, one mbarrier each;
+// 256 threads = 8 warps, each thread MX rows (8 apart) x 2 adjacent columns):
+//  * pulses go through shared memory in stages of PB pulses, two stages, one
+//    mbarrier per stage with PB arrivals.  For each pulse slot of the next
+//    stage one warp (slot mod 8) computes the (tile, pulse) geometry record in
+//    FP64 (tile-centre range, unit vector, phase and bin steps reduced mod 1)
+//    and issues one cp.async.bulk copy of the pulse's range-bin window (the
+//    bins any pixel of the tile can touch: +-|tile half-diagonal|), so the
+//    FP64 work and the copy issue are spread evenly over the warps;
 //  * range profiles live in HBM as pair entries {rc[b], rc[b+1]-rc[b]}
-//    (float4) so each pixel-pulse needs one 16-byte shared-memory load and
-//    two FMAs for the linear interpolation;
-//  * per pixel-pulse all arithmetic is FP32: the differential range is
-//    (Rc - R0) - u.d + g with the FP64 per-tile part carried as revolution
-//    and bin offsets, g = e (h + t hr) the far-field remainder (exact
-//    sqrt form for near-field pulses), phase reduced mod 1 before
-//    __sincosf, floor/fraction of the bin by a round-down add;
+//    (float4): one 16-byte shared-memory load and two FMAs interpolate;
+//  * per pixel-pulse all arithmetic is FP32: dR = (Rc - R0) - u.d + g with
+//    the FP64 per-tile part carried as a per-thread phase and bin base,
+//    g = e (h + t hr) the far-field remainder (exact sqrt form for near-field
+//    pulses); the phase stays in radians within a few multiples of pi of
+//    zero and goes straight to __sincosf; floor and fraction of the bin come
+//    from one round-down add whose result bits also form the shared-memory
+//    address;
 //  * complex64 results leave as float4 stores of two adjacent pixels.
 #include <cstdint>
 
@@ -34,9 +37,11 @@ namespace sarbp {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
 constexpr int kTY = 64;
-constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23
-constexpr int kRoundMagicBits = 0x4B400000;
+constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23: adding it rounds to an integer
+constexpr uint32_t kRoundMagicBits = 0x4B400000u;
+constexpr double kTwoPi = 6.283185307179586476925286766559;
 
 __device__ __forceinline__ PulseGeo make_geo(const BpLaunch &L, int p, double cx, double cy, double cz) {
     PulseGeo g;
@@ -56,27 +61,27 @@ __device__ __forceinline__ PulseGeo make_geo(const BpLaunch &L, int p, double cx
         return g;
     }
     const int ws = static_cast<int>(floor(bc)) - L.W;
-    g.ws = ws;
-    g.B0 = bc - static_cast<double>(ws);
-    g.A = frac_rev(kd);
     const double al = frac_rev(-k * ux * L.dx);
     const double be = frac_rev(-k * uy * L.dy);
+    g.A = frac_rev(kd);
     g.alpha = al;
     g.beta = be;
+    g.B0 = bc - static_cast<double>(ws);
     g.gam = -L.lambda * ux * L.dx;
     g.eta = -L.lambda * uy * L.dy;
-    g.a8 = static_cast<float>(frac_rev(8.0 * al));
-    g.b1 = static_cast<float>(be);
+    g.a8r = static_cast<float>(kTwoPi * frac_rev(8.0 * al));
+    g.b1r = static_cast<float>(kTwoPi * be);
     g.g8 = static_cast<float>(8.0 * g.gam);
     g.e1 = static_cast<float>(g.eta);
     g.tx = static_cast<float>(ux * L.dx);
     g.ty = static_cast<float>(uy * L.dy);
     g.h = static_cast<float>(0.5 * inv);
     g.hr = static_cast<float>(0.5 * inv * inv);
-    g.kappa = static_cast<float>(k);
+    g.kr = static_cast<float>(kTwoPi * k);
     g.rc = static_cast<float>(rc);
     g.lo = static_cast<float>(-ws);
     g.hi = static_cast<float>(L.nfft - 1 - ws);
+    g.ws = ws;
     int flags = 0;
     if (!(ws + L.wsize - 2 <= 0 || ws + 1 >= L.nfft - 1)) flags |= PG_ACTIVE;
     if (!(ws >= 0 && ws + L.wsize <= L.nfft)) flags |= PG_GATE;
@@ -85,80 +90,115 @@ __device__ __forceinline__ PulseGeo make_geo(const BpLaunch &L, int p, double cx
     return g;
 }
 
-// Warp 0: geometry of block b's pulses into geo_s, then one bulk copy per
-// active pulse of its window into win_s, all completing on `bar`.
+// Pulse slots of block b handled by this warp (slot q = warp, warp + 8, ...):
+// lane 0 writes the geometry record and either arrives with the window's byte
+// count and issues its bulk copy, or just arrives (inactive / past the end).
 template <int PB>
-__device__ __forceinline__ void produce_block(const BpLaunch &L, int b, PulseGeo *geo_s, float4 *win_s,
-                                              uint32_t bar, int lane, double cx, double cy, double cz) {
-    const int p = b * PB + lane;
-    uint32_t bytes = 0;
-    const float4 *src = nullptr;
-    if (lane < PB) {
+__device__ __forceinline__ void produce_slots(const BpLaunch &L, int b, PulseGeo *geo_s, uint32_t win_s,
+                                              uint32_t bar, int warp, int lane, double cx, double cy, double cz) {
+    if (lane != 0) return;
+    for (int q = warp; q < PB; q += kWarps) {
+        const int p = b * PB + q;
         PulseGeo g;
         g.flags = 0;
         if (p < L.np) g = make_geo(L, p, cx, cy, cz);
+        geo_s[q] = g;
         if (g.flags & PG_ACTIVE) {
-            bytes = static_cast<uint32_t>(L.wsize) * 16u;
-            src = static_cast<const float4 *>(L.pairs) + static_cast<long long>(p) * L.row_stride + L.guard + g.ws;
+            const uint32_t bytes = static_cast<uint32_t>(L.wsize) * 16u;
+            const float4 *src =
+                static_cast<const float4 *>(L.pairs) + static_cast<long long>(p) * L.row_stride + L.guard + g.ws;
+            mbar_arrive_expect_tx(bar, bytes);
+            bulk_copy_g2s(win_s + static_cast<uint32_t>(q) * bytes, src, bytes, bar);
+        } else {
+            mbar_arrive(bar);
         }
-        geo_s[lane] = g;
     }
-    const uint32_t total = __reduce_add_sync(0xffffffffu, bytes);
-    if (lane == 0) mbar_arrive_expect_tx(bar, total);
-    __syncwarp();
-    if (bytes) bulk_copy_g2s(smem_addr(win_s + lane * L.wsize), src, bytes, bar);
 }
 
+__device__ __forceinline__ float4 lds128(uint32_t addr) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "r"(addr));
+    return v;
+}
+
+__device__ __forceinline__ float2 splat(float a) { return make_float2(a, a); }
+
+// One pulse into the thread's MX x 2 pixels.  The two columns l = 0, 1 of a
+// row form a pair and all of their geometry arithmetic runs as paired FP32
+// instructions (__ffma2_rn and friends); the sine/cosine, the shared-memory
+// gather, the interpolation and the complex accumulate are per pixel.
+// Sign conventions avoid negations: nd2 = -|d|^2, so ne = t^2 - |d|^2 = -e,
+// ng = ne (h + t hr) = -g, and the phase / bin add -kr * ng, -lam * ng.
 template <int MX, bool GATE, bool NEAR, bool CHECKED>
-__device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, const float4 *__restrict__ w,
-                                                 const float4 *zero, int i0, int j0, float lam,
-                                                 const float (&d2)[MX][2], float (&acc_re)[MX][2],
-                                                 float (&acc_im)[MX][2], int wsize, unsigned *err) {
-    const double pd = fma(static_cast<double>(i0), g.alpha, fma(static_cast<double>(j0), g.beta, g.A));
-    const float P00 = static_cast<float>(pd - rint(pd));
-    const float B00 = static_cast<float>(fma(static_cast<double>(i0), g.gam, fma(static_cast<double>(j0), g.eta, g.B0)));
-    const float t00 = fmaf(static_cast<float>(i0), g.tx, static_cast<float>(j0) * g.ty);
-    const float tx8 = 8.0f * g.tx;
+__device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, uint32_t w_addr, uint32_t zero_addr, int i0,
+                                                 int j0, float lam, const float2 (&nd2)[MX],
+                                                 float (&acc_re)[MX][2], float (&acc_im)[MX][2], int wsize,
+                                                 unsigned *err) {
+    const double2 A_al = *reinterpret_cast<const double2 *>(&g.A);
+    const double2 be_B0 = *reinterpret_cast<const double2 *>(&g.beta);
+    const double2 ga_et = *reinterpret_cast<const double2 *>(&g.gam);
+    const float4 c0 = *reinterpret_cast<const float4 *>(&g.a8r);  // a8r, b1r, g8, e1
+    const float4 c1 = *reinterpret_cast<const float4 *>(&g.tx);   // tx, ty, h, hr
+    const float4 c2 = *reinterpret_cast<const float4 *>(&g.kr);   // kr, rc, lo, hi
+    // per-thread phase and bin base in FP64, phase reduced to [-pi, pi]
+    const double pd = fma(static_cast<double>(i0), A_al.y, fma(static_cast<double>(j0), be_B0.x, A_al.x));
+    const float P00 = static_cast<float>(kTwoPi * (pd - rint(pd)));
+    const float B00 =
+        static_cast<float>(fma(static_cast<double>(i0), ga_et.x, fma(static_cast<double>(j0), ga_et.y, be_B0.y)));
+    const float t00 = fmaf(static_cast<float>(i0), c1.x, static_cast<float>(j0) * c1.y);
+    float2 t2 = make_float2(t00, t00 + c1.y);
+    float2 Pb = make_float2(P00, P00 + c0.y);
+    float2 Bb = make_float2(B00, B00 + c0.w);
+    const float2 TX8 = splat(8.0f * c1.x), A8 = splat(c0.x), G8 = splat(c0.z);
+    const float2 HR = splat(c1.w), H = splat(c1.z), NKR = splat(-c2.x), NLAM = splat(-lam);
+    const float2 MAGIC = splat(kRoundMagic), NMAGIC = splat(-kRoundMagic), NEG1 = splat(-1.0f);
+    // shared address of pair entry floor(B): bits(B + 1.5*2^23, rounded down) * 16 + w_adj (mod 2^32)
+    const uint32_t w_adj = w_addr - kRoundMagicBits * 16u;
 #pragma unroll
     for (int k = 0; k < MX; ++k) {
-        const float Pk = fmaf(static_cast<float>(k), g.a8, P00);
-        const float Bk = fmaf(static_cast<float>(k), g.g8, B00);
-        const float tk = fmaf(static_cast<float>(k), tx8, t00);
+        if (k > 0) {
+            t2 = __fadd2_rn(t2, TX8);
+            Pb = __fadd2_rn(Pb, A8);
+            Bb = __fadd2_rn(Bb, G8);
+        }
+        float2 ng;
+        if (NEAR) {
+            const float e0 = -fmaf(t2.x, t2.x, nd2[k].x), e1 = -fmaf(t2.y, t2.y, nd2[k].y);
+            const float s0 = c2.y - t2.x, s1 = c2.y - t2.y;
+            ng = make_float2(-e0 / (s0 + sqrtf(fmaf(s0, s0, e0))), -e1 / (s1 + sqrtf(fmaf(s1, s1, e1))));
+        } else {
+            const float2 ne = __ffma2_rn(t2, t2, nd2[k]);
+            ng = __fmul2_rn(ne, __ffma2_rn(t2, HR, H));
+        }
+        const float2 P = __ffma2_rn(NKR, ng, Pb);
+        const float2 B = __ffma2_rn(NLAM, ng, Bb);
+        const float2 y = __fadd2_rd(B, MAGIC);
+        const float2 a = __ffma2_rn(__fadd2_rn(y, NMAGIC), NEG1, B);
 #pragma unroll
         for (int l = 0; l < 2; ++l) {
-            const float t = l ? tk + g.ty : tk;
-            const float Pb = l ? Pk + g.b1 : Pk;
-            const float Bb = l ? Bk + g.e1 : Bk;
-            const float e = fmaf(-t, t, d2[k][l]);
-            float gg;
-            if (NEAR) {
-                const float sv = g.rc - t;
-                gg = e / (sv + sqrtf(fmaf(sv, sv, e)));
-            } else {
-                gg = e * fmaf(t, g.hr, g.h);
-            }
-            const float P = fmaf(g.kappa, gg, Pb);
-            const float B = fmaf(lam, gg, Bb);
-            const float f = P - rintf(P);
+            const float Pl = l ? P.y : P.x;
+            const float Bl = l ? B.y : B.x;
+            const float yl = l ? y.y : y.x;
+            const float al = l ? a.y : a.x;
             float sn, cs;
-            __sincosf(6.28318530717958647692f * f, &sn, &cs);
-            const float y = __fadd_rd(B, kRoundMagic);
-            const float a = B - (y - kRoundMagic);
-            const int idx = __float_as_int(y) - kRoundMagicBits;
-            const float4 *src = w + idx;
+            __sincosf(Pl, &sn, &cs);
+            uint32_t addr = __float_as_uint(yl) * 16u + w_adj;
             if (GATE) {
-                const bool valid = (B > g.lo) && (B < g.hi);
-                src = valid ? src : zero;
+                const bool valid = (Bl > c2.z) && (Bl < c2.w);
+                addr = valid ? addr : zero_addr;
             }
             if (CHECKED) {
-                if (static_cast<unsigned>(idx) > static_cast<unsigned>(wsize - 2)) {
+                const uint32_t idx = __float_as_uint(yl) - kRoundMagicBits;
+                if (idx > static_cast<uint32_t>(wsize - 2)) {
                     atomicOr(err, ERRBIT_BOUNDS);
-                    src = zero;
+                    addr = zero_addr;
                 }
             }
-            const float4 v = *src;
-            const float re = fmaf(a, v.z, v.x);
-            const float im = fmaf(a, v.w, v.y);
+            const float4 v = lds128(addr);
+            const float re = fmaf(al, v.z, v.x);
+            const float im = fmaf(al, v.w, v.y);
             acc_re[k][l] = fmaf(re, cs, fmaf(-im, sn, acc_re[k][l]));
             acc_im[k][l] = fmaf(re, sn, fmaf(im, cs, acc_im[k][l]));
         }
@@ -172,8 +212,10 @@ __global__ void __launch_bounds__(kThreads, 2) bp_mixed_kernel(const BpLaunch L)
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     float4 *zero = reinterpret_cast<float4 *>(smem + 16);
     PulseGeo *geo = reinterpret_cast<PulseGeo *>(smem + 32);
-    float4 *win = reinterpret_cast<float4 *>(smem + 32 + 2 * PB * sizeof(PulseGeo));
+    const uint32_t win_addr = smem_addr(smem + 32 + 2 * PB * sizeof(PulseGeo));
+    const uint32_t zero_addr = smem_addr(zero);
     const int wsize = L.wsize;
+    const uint32_t pulse_bytes = static_cast<uint32_t>(wsize) * 16u;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ty0 = blockIdx.x * kTY, tx0 = blockIdx.y * TX, iz = blockIdx.z;
@@ -184,60 +226,74 @@ __global__ void __launch_bounds__(kThreads, 2) bp_mixed_kernel(const BpLaunch L)
     const int j0 = 2 * lane - kTY / 2;
     const float lam = static_cast<float>(L.lambda);
 
-    float d2[MX][2], acc_re[MX][2], acc_im[MX][2];
+    float2 nd2[MX];  // -|d|^2 of the thread's pixel pairs
+    float acc_re[MX][2], acc_im[MX][2];
     {
         const float dxf = static_cast<float>(L.dx), dyf = static_cast<float>(L.dy);
 #pragma unroll
-        for (int k = 0; k < MX; ++k)
+        for (int k = 0; k < MX; ++k) {
+            const float di = static_cast<float>(i0 + 8 * k) * dxf;
+            const float dj0 = static_cast<float>(j0) * dyf, dj1 = static_cast<float>(j0 + 1) * dyf;
+            nd2[k] = make_float2(-fmaf(di, di, dj0 * dj0), -fmaf(di, di, dj1 * dj1));
 #pragma unroll
             for (int l = 0; l < 2; ++l) {
-                const float di = static_cast<float>(i0 + 8 * k) * dxf;
-                const float dj = static_cast<float>(j0 + l) * dyf;
-                d2[k][l] = fmaf(di, di, dj * dj);
                 acc_re[k][l] = 0.0f;
                 acc_im[k][l] = 0.0f;
             }
+        }
     }
 
     const uint32_t bar_base = smem_addr(&bars[0]);  // stage s barrier at bar_base + 8*s
     if (threadIdx.x == 0) {
-        mbar_init(bar_base, 1);
-        mbar_init(bar_base + 8, 1);
+        mbar_init(bar_base, PB);
+        mbar_init(bar_base + 8, PB);
         *zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         fence_mbar_init();
     }
     __syncthreads();
 
     const int nblocks = (L.np + PB - 1) / PB;
-    if (warp == 0 && nblocks > 0) produce_block<PB>(L, 0, geo, win, bar_base, lane, cx, cy, cz);
+    if (nblocks > 0) produce_slots<PB>(L, 0, geo, win_addr, bar_base, warp, lane, cx, cy, cz);
     __syncthreads();
 
     int last_issued = 0;
     bool timed_out = false;
     for (int b = 0; b < nblocks; ++b) {
         const int s = b & 1;
-        if (warp == 0 && b + 1 < nblocks) {
-            produce_block<PB>(L, b + 1, geo + (s ^ 1) * PB, win + (s ^ 1) * PB * wsize, bar_base + 8 * (s ^ 1), lane, cx,
-                              cy, cz);
+        if (b + 1 < nblocks) {
+            produce_slots<PB>(L, b + 1, geo + (s ^ 1) * PB, win_addr + (s ^ 1) * PB * pulse_bytes,
+                              bar_base + 8 * (s ^ 1), warp, lane, cx, cy, cz);
             last_issued = b + 1;
         }
         const bool ok = mbar_wait_bounded(bar_base + 8 * s, (b >> 1) & 1, L.err);
         if (ok) {
             const int nq = min(PB, L.np - b * PB);
-            for (int q = 0; q < nq; ++q) {
-                const PulseGeo &g = geo[s * PB + q];
-                const int flags = g.flags;
-                if (!(flags & PG_ACTIVE)) continue;
-                const float4 *w = win + (s * PB + q) * wsize;
-                if (flags & PG_NEAR)
-                    accumulate_pulse<MX, true, true, CHECKED>(g, w, zero, i0, j0, lam, d2, acc_re, acc_im, wsize,
-                                                              L.err);
-                else if (flags & PG_GATE)
-                    accumulate_pulse<MX, true, false, CHECKED>(g, w, zero, i0, j0, lam, d2, acc_re, acc_im,
-                                                               wsize, L.err);
-                else
-                    accumulate_pulse<MX, false, false, CHECKED>(g, w, zero, i0, j0, lam, d2, acc_re, acc_im,
-                                                                wsize, L.err);
+            // stage summary: all PB pulses active, none gated or near-field
+            const int my_flags = lane < nq ? geo[s * PB + lane].flags : 0;
+            const int any_f = __reduce_or_sync(0xffffffffu, my_flags);
+            const int all_f = __reduce_and_sync(0xffffffffu, lane < nq ? my_flags : PG_ACTIVE);
+            const uint32_t w0 = win_addr + s * PB * pulse_bytes;
+            if (nq == PB && (all_f & PG_ACTIVE) && !(any_f & (PG_GATE | PG_NEAR))) {
+#pragma unroll
+                for (int q = 0; q < PB; ++q)
+                    accumulate_pulse<MX, false, false, CHECKED>(geo[s * PB + q], w0 + q * pulse_bytes, zero_addr,
+                                                                i0, j0, lam, nd2, acc_re, acc_im, wsize, L.err);
+            } else {
+                for (int q = 0; q < nq; ++q) {
+                    const PulseGeo &g = geo[s * PB + q];
+                    const int flags = g.flags;
+                    if (!(flags & PG_ACTIVE)) continue;
+                    const uint32_t w = w0 + q * pulse_bytes;
+                    if (flags & PG_NEAR)
+                        accumulate_pulse<MX, true, true, CHECKED>(g, w, zero_addr, i0, j0, lam, nd2, acc_re, acc_im,
+                                                                  wsize, L.err);
+                    else if (flags & PG_GATE)
+                        accumulate_pulse<MX, true, false, CHECKED>(g, w, zero_addr, i0, j0, lam, nd2, acc_re,
+                                                                   acc_im, wsize, L.err);
+                    else
+                        accumulate_pulse<MX, false, false, CHECKED>(g, w, zero_addr, i0, j0, lam, nd2, acc_re,
+                                                                    acc_im, wsize, L.err);
+                }
             }
         }
         if (__syncthreads_or(!ok)) {
@@ -248,7 +304,8 @@ __global__ void __launch_bounds__(kThreads, 2) bp_mixed_kernel(const BpLaunch L)
     if (timed_out) {
         // let the copies already issued for the other stage land before the
         // CTA's shared memory goes away (again bounded)
-        if (threadIdx.x == 0 && last_issued > 0) mbar_wait_bounded(bar_base + 8 * (last_issued & 1), (last_issued >> 1) & 1, L.err);
+        if (threadIdx.x == 0 && last_issued > 0)
+            mbar_wait_bounded(bar_base + 8 * (last_issued & 1), (last_issued >> 1) & 1, L.err);
         return;
     }
 
@@ -312,14 +369,21 @@ size_t bp_mixed_smem_bytes(const TileConfig &tc, int wsize) {
 cudaError_t launch_bp_mixed(const BpLaunch &L, const TileConfig &tc, bool checked, size_t smem, cudaStream_t s) {
 #define SARBP_MIXED_CASE(MX_, PB_) \
     if (tc.mx == MX_ && tc.pb == PB_) return launch_mx_pb<MX_, PB_>(L, checked, smem, s);
-    SARBP_MIXED_CASE(4, 4)
-    SARBP_MIXED_CASE(4, 8)
     SARBP_MIXED_CASE(4, 16)
-    SARBP_MIXED_CASE(2, 4)
-    SARBP_MIXED_CASE(2, 8)
+    SARBP_MIXED_CASE(4, 8)
+    SARBP_MIXED_CASE(4, 4)
+    SARBP_MIXED_CASE(4, 2)
+    SARBP_MIXED_CASE(4, 1)
     SARBP_MIXED_CASE(2, 16)
-    SARBP_MIXED_CASE(1, 8)
+    SARBP_MIXED_CASE(2, 8)
+    SARBP_MIXED_CASE(2, 4)
+    SARBP_MIXED_CASE(2, 2)
+    SARBP_MIXED_CASE(2, 1)
     SARBP_MIXED_CASE(1, 16)
+    SARBP_MIXED_CASE(1, 8)
+    SARBP_MIXED_CASE(1, 4)
+    SARBP_MIXED_CASE(1, 2)
+    SARBP_MIXED_CASE(1, 1)
 #undef SARBP_MIXED_CASE
     return cudaErrorInvalidValue;
 }
