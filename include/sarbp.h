@@ -176,6 +176,25 @@ SARBP_API int sarbp_focus_image(const sarbp_plan_desc *desc, const sarbp_apertur
  * return the first error they record (SARBP_OK if none). */
 SARBP_API int sarbp_plan_check(sarbp_plan *plan, void *stream);
 
+/* Backprojection for callers that cannot allocate device memory when they
+ * need an image (a pulse-callback loop that must not stall on cudaMalloc's
+ * device-wide synchronisation, an application that owns all GPU memory
+ * through its own pool or budget).  No counterpart in the reference.
+ * Inputs and output are device memory the caller owns: range profiles
+ * complex64 [num_pulses][nfft] (as sarbp_get_range_profiles returns them),
+ * geometry (memory must be SARBP_MEMORY_DEVICE), image complex64 on desc's
+ * grid.  desc supplies nfft, max_wr and the grid; precision must be
+ * SARBP_PRECISION_MIXED; flags may be SARBP_ACCUMULATE.  Allocates nothing:
+ * its scratch is a fixed 32 MiB file-scope device array per GPU, held until
+ * the process exits; requests whose staged rows, num_pulses x (nfft + 2 x
+ * (range-window + 2)) 16-byte entries, exceed 2^21 - 1 return
+ * SARBP_ERR_UNSUPPORTED.  The first call on a device looks up the array's
+ * address (make it before any stream capture).  Calls share the array:
+ * overlapping calls on the GPU race.  Synchronous: waits for the stream and
+ * returns kernel-side errors. */
+SARBP_API int sarbp_backproject_noalloc(const sarbp_plan_desc *desc, const void *range_profiles,
+                                        const sarbp_geometry *geometry, void *image, int flags, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,7 +37,7 @@ CHECKED = 2
 EXPORTED = (
     "sarbp_abi_version", "sarbp_status_string", "sarbp_plan_create", "sarbp_plan_destroy",
     "sarbp_plan_workspace_bytes", "sarbp_range_compress", "sarbp_get_range_profiles", "sarbp_backproject",
-    "sarbp_focus", "sarbp_focus_image", "sarbp_plan_check",
+    "sarbp_focus", "sarbp_focus_image", "sarbp_plan_check", "sarbp_backproject_noalloc",
 )
 
 
@@ -86,6 +86,7 @@ def lib():
         L.sarbp_focus.argtypes = [vp, P(Aperture), vp, i, vp]
         L.sarbp_focus_image.argtypes = [P(PlanDesc), P(Aperture), vp, i]
         L.sarbp_plan_check.argtypes = [vp, vp]
+        L.sarbp_backproject_noalloc.argtypes = [P(PlanDesc), vp, P(Geometry), vp, i, vp]
         for name in EXPORTED:
             if name != "sarbp_status_string":
                 getattr(L, name).restype = i
