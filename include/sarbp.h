@@ -168,6 +168,21 @@ SARBP_API int sarbp_backproject(sarbp_plan *plan, const sarbp_geometry *geometry
 SARBP_API int sarbp_focus(sarbp_plan *plan, const sarbp_aperture *aperture, void *image, int image_memory,
                 void *stream);
 
+/* Gradient of a real image loss with respect to the per-pulse geometry
+ * (the adjoint of the backprojection with respect to antenna position and
+ * slant range; no counterpart in the reference, whose autofocus searches a
+ * grid instead, src/autofocus/autofocus_gpu.cu:707-1260).  Uses the plan's
+ * current range profiles and the same geometry as the forward call.
+ * grad_image: dL/dRe(img) + j dL/dIm(img), complex64 on the plan's grid
+ * (SARBP_PRECISION_MIXED plans).  Outputs: grad_ant double [3][num_pulses]
+ * (rows d/dant_x, d/dant_y, d/dant_z), grad_r0 double [num_pulses] or NULL.
+ * flags: SARBP_ACCUMULATE adds into the outputs.  Nothing per pixel-pulse is
+ * stored; ranges are recomputed per tile.  The first call allocates the
+ * per-tile partial buffer. */
+SARBP_API int sarbp_backproject_adjoint(sarbp_plan *plan, const sarbp_geometry *geometry, const void *grad_image,
+                                        int grad_memory, double *grad_ant, double *grad_r0, int out_memory,
+                                        int flags, void *stream);
+
 /* One call, no plan kept: create, focus, destroy (host or device buffers). */
 SARBP_API int sarbp_focus_image(const sarbp_plan_desc *desc, const sarbp_aperture *aperture, void *image,
                       int image_memory);

@@ -417,3 +417,78 @@ int oracle_bp_ref32(int Np, int nfft, const float *rc, const float *ax, const fl
     free(ty);
     return 0;
 }
+
+/* ------------------------------------------------------------------------- */
+/* gradient of a real image loss with respect to the pulse geometry, FP64     */
+/* ------------------------------------------------------------------------- */
+
+/*
+ * For img_q = sum_p v_p(b_pq) exp(j phi_pq) (bp_pixel_fp64 above) and the
+ * upstream gradient G_q = dL/dRe(img_q) + j dL/dIm(img_q):
+ *   s_pq = Re(conj(G_q) (lambda v'_p(b) + j 2 pi k_p v_p(b)) exp(j phi_pq)),
+ *   dL/da_p = sum_q s_pq (a_p - x_q)/|a_p - x_q|,   dL/dR0_p = -sum_q s_pq,
+ * with lambda = nfft / max_wr, k_p = 2 f0_p / c and v'_p the slope of the
+ * linear interpolation on the bracket interp1 selects.  G and the image are
+ * [nz][nx][ny]; outputs are double [Np].  There is no reference counterpart
+ * (the reference's autofocus is a grid search); this is the exact derivative
+ * of the FP64 forward restatement, used to check the GPU adjoint.
+ */
+int oracle_bp_grad_fp64(int Np, int nfft, const double *rc, const double *ax, const double *ay, const double *az,
+                        const double *r0, const double *f0, double max_wr, int nx, int ny, int nz, double x0,
+                        double y0, double z0, double wx, double wy, double wz, const double *G, double *gax,
+                        double *gay, double *gaz, double *gr0) {
+    if (Np <= 0 || nfft < 2 || nx <= 0 || ny <= 0 || nz <= 0 || !rc || !G || !gax || !gay || !gaz) return -1;
+    double *r_vec = make_rvec_fp64(nfft, max_wr);
+    if (!r_vec) return -2;
+    const double rmin = r_vec[0], rmax = r_vec[nfft - 1];
+    const double lam = (double)nfft / max_wr;
+    const long long nxy = (long long)nx * ny;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int p = 0; p < Np; p++) {
+        const double k = 2.0 * f0[p] / ORACLE_CLIGHT;
+        double sx = 0.0, sy = 0.0, sz = 0.0, s0 = 0.0;
+        for (int iz = 0; iz < nz; iz++) {
+            const double z = grid_coord(iz, nz, z0, wz);
+            for (int ix = 0; ix < nx; ix++) {
+                const double x = grid_coord(ix, nx, x0, wx);
+                for (int iy = 0; iy < ny; iy++) {
+                    const double y = grid_coord(iy, ny, y0, wy);
+                    const double dx = ax[p] - x, dy = ay[p] - y, dz = az[p] - z;
+                    const double R = sqrt(dx * dx + dy * dy + dz * dz);
+                    const double dR = R - r0[p];
+                    if (!(dR > rmin && dR < rmax)) continue;
+                    const double idx = (dR / max_wr + 0.5) * (double)nfft;
+                    int right = (int)floor(idx) - 1;
+                    if (right < -1) right = -1;
+                    while (++right < nfft && r_vec[right] <= dR) {
+                    }
+                    if (right == nfft || right == 0) continue;
+                    const double alpha = (dR - r_vec[right - 1]) / (r_vec[right] - r_vec[right - 1]);
+                    const double *lo = rc + 2 * ((size_t)p * nfft + right - 1);
+                    const double *hi = rc + 2 * ((size_t)p * nfft + right);
+                    const double vr = alpha * hi[0] + (1.0 - alpha) * lo[0];
+                    const double vi = alpha * hi[1] + (1.0 - alpha) * lo[1];
+                    const double dr = hi[0] - lo[0], di = hi[1] - lo[1];
+                    const double phi = 4.0 * ORACLE_PI * f0[p] * dR / ORACLE_CLIGHT;
+                    const double c = cos(phi), s = sin(phi);
+                    /* D = (lambda v' + j 2 pi k v) exp(j phi) */
+                    const double pr = lam * dr - 2.0 * ORACLE_PI * k * vi;
+                    const double pi_ = lam * di + 2.0 * ORACLE_PI * k * vr;
+                    const double Dr = pr * c - pi_ * s, Di = pr * s + pi_ * c;
+                    const long long o = (long long)iz * nxy + (long long)ix * ny + iy;
+                    const double sv = G[2 * o] * Dr + G[2 * o + 1] * Di; /* Re(conj(G) D) */
+                    sx += sv * dx / R;
+                    sy += sv * dy / R;
+                    sz += sv * dz / R;
+                    s0 += sv;
+                }
+            }
+        }
+        gax[p] = sx;
+        gay[p] = sy;
+        gaz[p] = sz;
+        if (gr0) gr0[p] = -s0;
+    }
+    free(r_vec);
+    return 0;
+}

@@ -50,10 +50,11 @@ def lib():
         L.oracle_range_compress_ref64.argtypes = [_c.c_int, _c.c_int, _f64p, _f64p]
         L.oracle_bp_ref64.argtypes = ([_c.c_int, _c.c_int, _f64p] + [_f64p] * 5 + [_c.c_double, _c.c_int, _c.c_int]
                                       + [_c.c_double] * 4 + [_f64p])
+        L.oracle_bp_grad_fp64.argtypes = ([_c.c_int, _c.c_int, _f64p] + bp_geo + [_f64p] * 5)
         L.oracle_dft_c128.argtypes = [_c.c_int, _f64p, _f64p, _c.c_int]
         for f in ("oracle_range_compress_fp64", "oracle_range_compress_ref32", "oracle_bp_fp64",
                   "oracle_bp_fp64_pixels", "oracle_bp_ref32", "oracle_dft_c128", "oracle_range_compress_ref64",
-                  "oracle_bp_ref64"):
+                  "oracle_bp_ref64", "oracle_bp_grad_fp64"):
             getattr(L, f).restype = _c.c_int
         _LIB = L
     return _LIB
@@ -141,6 +142,20 @@ def bp_fp64_pixels(rc: np.ndarray, ax, ay, az, r0, f0, max_wr: float, grid, pix:
                                        grid.wx, grid.wy, grid.wz, pix.shape[0], pix,
                                        out.view(np.float64).reshape(-1)), "bp_fp64_pixels")
     return out
+
+
+def bp_grad_fp64(rc: np.ndarray, ax, ay, az, r0, f0, max_wr: float, grid, G: np.ndarray):
+    """dL/d(ant_x, ant_y, ant_z) [3, Np] and dL/dR0 [Np] of a loss with upstream
+    image gradient G (complex, [nz, nx, ny])."""
+    rc = np.ascontiguousarray(rc, dtype=np.complex128)
+    Np, nfft = rc.shape
+    G = np.ascontiguousarray(G, dtype=np.complex128)
+    out = np.zeros((4, Np), dtype=np.float64)
+    _check(lib().oracle_bp_grad_fp64(Np, nfft, rc.view(np.float64).reshape(-1), *_geo(ax, ay, az, r0, f0),
+                                     float(max_wr), grid.nx, grid.ny, grid.nz, grid.x0, grid.y0, grid.z0, grid.wx,
+                                     grid.wy, grid.wz, G.view(np.float64).reshape(-1), out[0], out[1], out[2],
+                                     out[3]), "bp_grad_fp64")
+    return out[:3], out[3]
 
 
 def focus_fp64(scene, pixels: Optional[np.ndarray] = None) -> np.ndarray:

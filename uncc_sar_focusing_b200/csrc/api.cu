@@ -148,6 +148,8 @@ void release(sarbp_plan *p) {
     cudaFree(p->d_fac);
     cudaFree(p->d_img);
     cudaFree(p->d_err);
+    cudaFree(p->d_partials);
+    cudaFree(p->d_gout);
     delete p;
 }
 
@@ -208,40 +210,9 @@ int range_compress_impl(sarbp_plan *p, const void *ph, int np, int memory, cudaS
     return SARBP_OK;
 }
 
-int backproject_impl(sarbp_plan *p, const sarbp_geometry *geo, void *image, int image_memory, int flags,
-                     cudaStream_t s) {
-    if (!geo || !image || !geo->ant_x || !geo->ant_y || !geo->ant_z || !geo->slant_range || !geo->start_freq)
-        return SARBP_ERR_NULL_POINTER;
-    if (geo->num_pulses < 1 || geo->num_pulses > p->np_ready) return SARBP_ERR_INVALID_ARGUMENT;
-    if ((geo->memory != SARBP_MEMORY_HOST && geo->memory != SARBP_MEMORY_DEVICE) ||
-        (image_memory != SARBP_MEMORY_HOST && image_memory != SARBP_MEMORY_DEVICE) ||
-        (flags & ~(SARBP_ACCUMULATE | SARBP_CHECKED)))
-        return SARBP_ERR_INVALID_ARGUMENT;
-    const int np = geo->num_pulses;
-    const double *ax = geo->ant_x, *ay = geo->ant_y, *az = geo->ant_z, *r0 = geo->slant_range,
-                 *f0 = geo->start_freq;
-    if (geo->memory == SARBP_MEMORY_HOST) {
-        const int st = check_geometry_host(geo);
-        if (st != SARBP_OK) return st;
-        const double *src[5] = {ax, ay, az, r0, f0};
-        for (int i = 0; i < 5; ++i)
-            SARBP_TRY_CUDA(cudaMemcpyAsync(p->d_geo + static_cast<size_t>(i) * p->np_cap, src[i],
-                                           sizeof(double) * np, cudaMemcpyHostToDevice, s));
-        ax = p->d_geo;
-        ay = p->d_geo + p->np_cap;
-        az = p->d_geo + 2 * p->np_cap;
-        r0 = p->d_geo + 3 * p->np_cap;
-        f0 = p->d_geo + 4 * p->np_cap;
-    }
+BpLaunch launch_params(const sarbp_plan *p, const double *ax, const double *ay, const double *az, const double *r0,
+                       const double *f0, int np, void *img, int flags) {
     const sarbp_grid &g = p->desc.grid;
-    const size_t img_bytes = static_cast<size_t>(g.nx) * g.ny * g.nz * cplx_bytes(p);
-    void *dimg = image;
-    if (image_memory == SARBP_MEMORY_HOST) {
-        dimg = p->d_img;
-        if (flags & SARBP_ACCUMULATE)
-            SARBP_TRY_CUDA(cudaMemcpyAsync(dimg, image, img_bytes, cudaMemcpyHostToDevice, s));
-    }
-
     BpLaunch L{};
     L.pairs = p->d_pairs;
     L.row_stride = p->row_stride;
@@ -268,10 +239,55 @@ int backproject_impl(sarbp_plan *p, const sarbp_geometry *geo, void *image, int 
     L.wsize = p->wsize;
     L.near_hd16 = p->near_hd16;
     L.near_coef = p->near_coef;
-    L.img = dimg;
+    L.img = img;
     L.accumulate = (flags & SARBP_ACCUMULATE) ? 1 : 0;
-    L.vec_store = ((reinterpret_cast<uintptr_t>(dimg) & 15u) == 0 && (g.ny % 2) == 0) ? 1 : 0;
+    L.vec_store = ((reinterpret_cast<uintptr_t>(img) & 15u) == 0 && (g.ny % 2) == 0) ? 1 : 0;
     L.err = p->d_err;
+    return L;
+}
+
+// Geometry arrays on the device: the caller's, or the plan's staging copy.
+int device_geometry(sarbp_plan *p, const sarbp_geometry *geo, cudaStream_t s, const double **out) {
+    const int np = geo->num_pulses;
+    const double *src[5] = {geo->ant_x, geo->ant_y, geo->ant_z, geo->slant_range, geo->start_freq};
+    if (geo->memory == SARBP_MEMORY_HOST) {
+        const int st = check_geometry_host(geo);
+        if (st != SARBP_OK) return st;
+        for (int i = 0; i < 5; ++i) {
+            SARBP_TRY_CUDA(cudaMemcpyAsync(p->d_geo + static_cast<size_t>(i) * p->np_cap, src[i],
+                                           sizeof(double) * np, cudaMemcpyHostToDevice, s));
+            out[i] = p->d_geo + static_cast<size_t>(i) * p->np_cap;
+        }
+    } else {
+        for (int i = 0; i < 5; ++i) out[i] = src[i];
+    }
+    return SARBP_OK;
+}
+
+int backproject_impl(sarbp_plan *p, const sarbp_geometry *geo, void *image, int image_memory, int flags,
+                     cudaStream_t s) {
+    if (!geo || !image || !geo->ant_x || !geo->ant_y || !geo->ant_z || !geo->slant_range || !geo->start_freq)
+        return SARBP_ERR_NULL_POINTER;
+    if (geo->num_pulses < 1 || geo->num_pulses > p->np_ready) return SARBP_ERR_INVALID_ARGUMENT;
+    if ((geo->memory != SARBP_MEMORY_HOST && geo->memory != SARBP_MEMORY_DEVICE) ||
+        (image_memory != SARBP_MEMORY_HOST && image_memory != SARBP_MEMORY_DEVICE) ||
+        (flags & ~(SARBP_ACCUMULATE | SARBP_CHECKED)))
+        return SARBP_ERR_INVALID_ARGUMENT;
+    const int np = geo->num_pulses;
+    const double *gp[5];
+    const int gst = device_geometry(p, geo, s, gp);
+    if (gst != SARBP_OK) return gst;
+    const double *ax = gp[0], *ay = gp[1], *az = gp[2], *r0 = gp[3], *f0 = gp[4];
+    const sarbp_grid &g = p->desc.grid;
+    const size_t img_bytes = static_cast<size_t>(g.nx) * g.ny * g.nz * cplx_bytes(p);
+    void *dimg = image;
+    if (image_memory == SARBP_MEMORY_HOST) {
+        dimg = p->d_img;
+        if (flags & SARBP_ACCUMULATE)
+            SARBP_TRY_CUDA(cudaMemcpyAsync(dimg, image, img_bytes, cudaMemcpyHostToDevice, s));
+    }
+
+    BpLaunch L = launch_params(p, ax, ay, az, r0, f0, np, dimg, flags);
     cudaError_t e;
     if (p->precision == SARBP_PRECISION_FP64)
         e = launch_bp_fp64(L, p->tile, p->smem, s);
@@ -283,6 +299,72 @@ int backproject_impl(sarbp_plan *p, const sarbp_geometry *geo, void *image, int 
         return read_errors(p, s);
     }
     if (geo->memory == SARBP_MEMORY_HOST) SARBP_TRY_CUDA(cudaStreamSynchronize(s));
+    return SARBP_OK;
+}
+
+int adjoint_impl(sarbp_plan *p, const sarbp_geometry *geo, const void *grad, int grad_memory, double *grad_ant,
+                 double *grad_r0, int out_memory, int flags, cudaStream_t s) {
+    if (!geo || !grad || !grad_ant || !geo->ant_x || !geo->ant_y || !geo->ant_z || !geo->slant_range ||
+        !geo->start_freq)
+        return SARBP_ERR_NULL_POINTER;
+    if (p->precision != SARBP_PRECISION_MIXED) return SARBP_ERR_UNSUPPORTED;
+    if (geo->num_pulses < 1 || geo->num_pulses > p->np_ready) return SARBP_ERR_INVALID_ARGUMENT;
+    if ((geo->memory != SARBP_MEMORY_HOST && geo->memory != SARBP_MEMORY_DEVICE) ||
+        (grad_memory != SARBP_MEMORY_HOST && grad_memory != SARBP_MEMORY_DEVICE) ||
+        (out_memory != SARBP_MEMORY_HOST && out_memory != SARBP_MEMORY_DEVICE) || (flags & ~SARBP_ACCUMULATE))
+        return SARBP_ERR_INVALID_ARGUMENT;
+    const int np = geo->num_pulses;
+    const double *gp[5];
+    const int gst = device_geometry(p, geo, s, gp);
+    if (gst != SARBP_OK) return gst;
+    const sarbp_grid &g = p->desc.grid;
+    const size_t npix = static_cast<size_t>(g.nx) * g.ny * g.nz;
+    const void *dgrad = grad;
+    if (grad_memory == SARBP_MEMORY_HOST) {
+        SARBP_TRY_CUDA(cudaMemcpyAsync(p->d_img, grad, npix * 8, cudaMemcpyHostToDevice, s));
+        dgrad = p->d_img;
+    }
+    // stage depth: the deepest of 4, 2, 1 pulses whose shared memory fits
+    TileConfig tc{p->tile.mx, 4};
+    size_t smem = bp_adjoint_smem_bytes(tc, p->wsize);
+    while (tc.pb > 1 && smem > 110u * 1024u) {
+        tc.pb /= 2;
+        smem = bp_adjoint_smem_bytes(tc, p->wsize);
+    }
+    if (smem > 227u * 1024u) return SARBP_ERR_UNSUPPORTED;
+    BpLaunch L = launch_params(p, gp[0], gp[1], gp[2], gp[3], gp[4], np, nullptr, 0);
+    const long long ntiles = bp_tile_count(L, tc);
+    const size_t need = static_cast<size_t>(ntiles) * p->np_cap * 16;
+    if (p->partials_bytes < need) {
+        cudaFree(p->d_partials);
+        p->d_partials = nullptr;
+        p->partials_bytes = 0;
+        const int st = alloc(p, &p->d_partials, need);
+        if (st != SARBP_OK) return st;
+        p->partials_bytes = need;
+    }
+    double *gant = grad_ant, *gr0 = grad_r0;
+    if (out_memory == SARBP_MEMORY_HOST) {
+        if (!p->d_gout) {
+            const int st = alloc(p, reinterpret_cast<void **>(&p->d_gout), 4 * sizeof(double) * p->np_cap);
+            if (st != SARBP_OK) return st;
+        }
+        gant = p->d_gout;
+        gr0 = grad_r0 ? p->d_gout + 3 * np : nullptr;
+        if (flags & SARBP_ACCUMULATE) {
+            SARBP_TRY_CUDA(cudaMemcpyAsync(gant, grad_ant, 3 * sizeof(double) * np, cudaMemcpyHostToDevice, s));
+            if (gr0) SARBP_TRY_CUDA(cudaMemcpyAsync(gr0, grad_r0, sizeof(double) * np, cudaMemcpyHostToDevice, s));
+        }
+    }
+    SARBP_TRY_CUDA(launch_bp_adjoint(L, dgrad, p->d_partials, tc, smem, s));
+    SARBP_TRY_CUDA(launch_adjoint_reduce(p->d_partials, ntiles, np, gant, gr0, (flags & SARBP_ACCUMULATE) ? 1 : 0, s));
+    if (out_memory == SARBP_MEMORY_HOST) {
+        SARBP_TRY_CUDA(cudaMemcpyAsync(grad_ant, gant, 3 * sizeof(double) * np, cudaMemcpyDeviceToHost, s));
+        if (grad_r0) SARBP_TRY_CUDA(cudaMemcpyAsync(grad_r0, gr0, sizeof(double) * np, cudaMemcpyDeviceToHost, s));
+        return read_errors(p, s);
+    }
+    if (geo->memory == SARBP_MEMORY_HOST || grad_memory == SARBP_MEMORY_HOST)
+        SARBP_TRY_CUDA(cudaStreamSynchronize(s));
     return SARBP_OK;
 }
 
@@ -475,6 +557,16 @@ int sarbp_focus_image(const sarbp_plan_desc *desc, const sarbp_aperture *ap, voi
     if (st == SARBP_OK) st = sarbp_plan_check(plan, nullptr);
     sarbp_plan_destroy(plan);
     return st;
+}
+
+int sarbp_backproject_adjoint(sarbp_plan *plan, const sarbp_geometry *geometry, const void *grad_image,
+                              int grad_memory, double *grad_ant, double *grad_r0, int out_memory, int flags,
+                              void *stream) {
+    if (!plan) return SARBP_ERR_NULL_POINTER;
+    DeviceGuard guard(plan->device);
+    SARBP_TRY_CUDA(guard.status);
+    return adjoint_impl(plan, geometry, grad_image, grad_memory, grad_ant, grad_r0, out_memory, flags,
+                        static_cast<cudaStream_t>(stream));
 }
 
 int sarbp_plan_check(sarbp_plan *plan, void *stream) {

@@ -119,8 +119,9 @@ struct __align__(16) PulseGeo {
     int ws;                  // window start bin (may be negative: guard band)
     int flags;               // PG_*
     int pad0, pad1;
+    float ux, uy, uz, rinv;  // unit vector tile centre -> antenna, 1/Rc (adjoint kernel)
 };
-static_assert(sizeof(PulseGeo) == 112, "PulseGeo layout");
+static_assert(sizeof(PulseGeo) == 128, "PulseGeo layout");
 
 // Geometry of one pulse for the FP64 kernel (per-pixel exact computation).
 struct __align__(16) PulseGeo64 {

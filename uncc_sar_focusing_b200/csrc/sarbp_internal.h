@@ -40,6 +40,14 @@ cudaError_t launch_bp_mixed(const BpLaunch &L, const TileConfig &tc, bool checke
                             cudaStream_t s);
 cudaError_t launch_bp_fp64(const BpLaunch &L, const TileConfig &tc, size_t smem, cudaStream_t s);
 size_t bp_mixed_smem_bytes(const TileConfig &tc, int wsize);
+// Adjoint (bp_adjoint.cu): per-(tile, pulse) gradient partials, then a sum
+// over tiles into grad_ant [3][np] and grad_r0 [np].
+cudaError_t launch_bp_adjoint(const BpLaunch &L, const void *grad, void *partials, const TileConfig &tc, size_t smem,
+                              cudaStream_t s);
+cudaError_t launch_adjoint_reduce(const void *partials, long long ntiles, int np, double *grad_ant, double *grad_r0,
+                                  int accumulate, cudaStream_t s);
+size_t bp_adjoint_smem_bytes(const TileConfig &tc, int wsize);
+long long bp_tile_count(const BpLaunch &L, const TileConfig &tc);
 size_t bp_fp64_smem_bytes(const TileConfig &tc, int wsize);
 
 // Range compression kernels (range_compress.cu)
@@ -69,6 +77,9 @@ struct sarbp_plan {
     void *d_fac;      // per-sample window * scale * shift twiddle [K]
     void *d_img;      // image staging for host outputs
     unsigned *d_err;  // device error bits
+    void *d_partials; // adjoint per-(tile, pulse) partial gradients (allocated on first use)
+    size_t partials_bytes;
+    double *d_gout;   // adjoint output staging for host outputs [4][np] (allocated on first use)
     size_t bytes;     // device bytes held
     cufftHandle fft;
     bool fft_ok;

@@ -159,6 +159,28 @@ class Plan:
             np.copyto(out, ikeep.reshape(out.shape))
         return out
 
+    def backproject_adjoint(self, ant_x, ant_y, ant_z, slant_range, start_freq, grad_image, accumulate=False):
+        """dL/d(ant_x, ant_y, ant_z) as a [3, Np] array and dL/dR0 [Np] for a
+        real loss L whose image gradient is grad_image = dL/dRe + j dL/dIm
+        (sarbp_backproject_adjoint, on the plan's current range profiles)."""
+        geo, keep = self._geometry(ant_x, ant_y, ant_z, slant_range, start_freq)
+        gp, gmem, gkeep = _ptr(grad_image, np.complex64, int(np.prod(self.image_shape())))
+        n = geo.num_pulses
+        if gmem == N.MEMORY_DEVICE:
+            import torch
+
+            gant = torch.zeros((3, n), dtype=torch.float64, device=grad_image.device)
+            gr0 = torch.zeros(n, dtype=torch.float64, device=grad_image.device)
+            optr = (ctypes.c_void_p(gant.data_ptr()), ctypes.c_void_p(gr0.data_ptr()))
+        else:
+            gant = np.zeros((3, n), dtype=np.float64)
+            gr0 = np.zeros(n, dtype=np.float64)
+            optr = (ctypes.c_void_p(gant.ctypes.data), ctypes.c_void_p(gr0.ctypes.data))
+        st = N.lib().sarbp_backproject_adjoint(self._h, ctypes.byref(geo), gp, gmem, optr[0], optr[1], gmem,
+                                               N.ACCUMULATE if accumulate else 0, _stream(grad_image, ant_x))
+        N.check(st, "sarbp_backproject_adjoint")
+        return gant, gr0
+
     def focus(self, phase_history, ant_x, ant_y, ant_z, slant_range, start_freq, out=None):
         geo, keep = self._geometry(ant_x, ant_y, ant_z, slant_range, start_freq)
         if int(phase_history.shape[0]) != geo.num_pulses:
