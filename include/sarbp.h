@@ -164,6 +164,15 @@ SARBP_API int sarbp_get_range_profiles(sarbp_plan *plan, void *out, int memory, 
 SARBP_API int sarbp_backproject(sarbp_plan *plan, const sarbp_geometry *geometry, void *image, int image_memory,
                       int flags, void *stream);
 
+/* Backprojection of the plan's range profiles for num_hypotheses antenna
+ * tracks at once (one launch; SARBP_PRECISION_MIXED plans).  The geometry
+ * arrays hold num_hypotheses x num_pulses values, hypothesis-major; images is
+ * complex64 [num_hypotheses][nz][nx][ny].  Used for motion-hypothesis batches
+ * and search-based autofocus, where the reference evaluates one full image
+ * per grid point (src/autofocus/gridSearchErrorFunctions_dft.cuh:258-336). */
+SARBP_API int sarbp_backproject_hypotheses(sarbp_plan *plan, const sarbp_geometry *geometry, int num_hypotheses,
+                                           void *images, int image_memory, int flags, void *stream);
+
 /* Range compression + backprojection: the reference's cuda_focus_SAR_image. */
 SARBP_API int sarbp_focus(sarbp_plan *plan, const sarbp_aperture *aperture, void *image, int image_memory,
                 void *stream);

@@ -150,6 +150,7 @@ void release(sarbp_plan *p) {
     cudaFree(p->d_err);
     cudaFree(p->d_partials);
     cudaFree(p->d_gout);
+    cudaFree(p->d_hyp);
     delete p;
 }
 
@@ -243,6 +244,7 @@ BpLaunch launch_params(const sarbp_plan *p, const double *ax, const double *ay, 
     L.accumulate = (flags & SARBP_ACCUMULATE) ? 1 : 0;
     L.vec_store = ((reinterpret_cast<uintptr_t>(img) & 15u) == 0 && (g.ny % 2) == 0) ? 1 : 0;
     L.err = p->d_err;
+    L.nhyp = 1;
     return L;
 }
 
@@ -296,6 +298,60 @@ int backproject_impl(sarbp_plan *p, const sarbp_geometry *geo, void *image, int 
     SARBP_TRY_CUDA(e);
     if (image_memory == SARBP_MEMORY_HOST) {
         SARBP_TRY_CUDA(cudaMemcpyAsync(image, dimg, img_bytes, cudaMemcpyDeviceToHost, s));
+        return read_errors(p, s);
+    }
+    if (geo->memory == SARBP_MEMORY_HOST) SARBP_TRY_CUDA(cudaStreamSynchronize(s));
+    return SARBP_OK;
+}
+
+int hypotheses_impl(sarbp_plan *p, const sarbp_geometry *geo, int nhyp, void *images, int image_memory, int flags,
+                    cudaStream_t s) {
+    if (!geo || !images || !geo->ant_x || !geo->ant_y || !geo->ant_z || !geo->slant_range || !geo->start_freq)
+        return SARBP_ERR_NULL_POINTER;
+    if (p->precision != SARBP_PRECISION_MIXED) return SARBP_ERR_UNSUPPORTED;
+    const sarbp_grid &g = p->desc.grid;
+    if (nhyp < 1 || static_cast<long long>(nhyp) * g.nz > 65535 || geo->num_pulses < 1 ||
+        geo->num_pulses > p->np_ready || (geo->memory != SARBP_MEMORY_HOST && geo->memory != SARBP_MEMORY_DEVICE) ||
+        (image_memory != SARBP_MEMORY_HOST && image_memory != SARBP_MEMORY_DEVICE) || (flags & ~SARBP_ACCUMULATE))
+        return SARBP_ERR_INVALID_ARGUMENT;
+    const int np = geo->num_pulses;
+    const size_t ngeo = static_cast<size_t>(nhyp) * np;
+    const size_t img_bytes = static_cast<size_t>(nhyp) * g.nx * g.ny * g.nz * 8;
+    const double *src[5] = {geo->ant_x, geo->ant_y, geo->ant_z, geo->slant_range, geo->start_freq};
+    const double *dg[5];
+    const size_t need = (geo->memory == SARBP_MEMORY_HOST ? 5 * ngeo * sizeof(double) : 0) +
+                        (image_memory == SARBP_MEMORY_HOST ? img_bytes : 0);
+    if (need > p->hyp_bytes) {
+        cudaFree(p->d_hyp);
+        p->d_hyp = nullptr;
+        p->hyp_bytes = 0;
+        const int st = alloc(p, &p->d_hyp, need);
+        if (st != SARBP_OK) return st;
+        p->hyp_bytes = need;
+    }
+    unsigned char *stage = static_cast<unsigned char *>(p->d_hyp);
+    if (geo->memory == SARBP_MEMORY_HOST) {
+        for (int i = 0; i < 5; ++i) {
+            for (size_t j = 0; j < ngeo; ++j)
+                if (!std::isfinite(src[i][j])) return SARBP_ERR_NOT_FINITE;
+            double *d = reinterpret_cast<double *>(stage) + i * ngeo;
+            SARBP_TRY_CUDA(cudaMemcpyAsync(d, src[i], ngeo * sizeof(double), cudaMemcpyHostToDevice, s));
+            dg[i] = d;
+        }
+        stage += 5 * ngeo * sizeof(double);
+    } else {
+        for (int i = 0; i < 5; ++i) dg[i] = src[i];
+    }
+    void *dimg = images;
+    if (image_memory == SARBP_MEMORY_HOST) {
+        dimg = stage;
+        if (flags & SARBP_ACCUMULATE) SARBP_TRY_CUDA(cudaMemcpyAsync(dimg, images, img_bytes, cudaMemcpyHostToDevice, s));
+    }
+    BpLaunch L = launch_params(p, dg[0], dg[1], dg[2], dg[3], dg[4], np, dimg, flags);
+    L.nhyp = nhyp;
+    SARBP_TRY_CUDA(launch_bp_mixed(L, p->tile, false, p->smem, s));
+    if (image_memory == SARBP_MEMORY_HOST) {
+        SARBP_TRY_CUDA(cudaMemcpyAsync(images, dimg, img_bytes, cudaMemcpyDeviceToHost, s));
         return read_errors(p, s);
     }
     if (geo->memory == SARBP_MEMORY_HOST) SARBP_TRY_CUDA(cudaStreamSynchronize(s));
@@ -557,6 +613,15 @@ int sarbp_focus_image(const sarbp_plan_desc *desc, const sarbp_aperture *ap, voi
     if (st == SARBP_OK) st = sarbp_plan_check(plan, nullptr);
     sarbp_plan_destroy(plan);
     return st;
+}
+
+int sarbp_backproject_hypotheses(sarbp_plan *plan, const sarbp_geometry *geometry, int num_hypotheses, void *images,
+                                 int image_memory, int flags, void *stream) {
+    if (!plan) return SARBP_ERR_NULL_POINTER;
+    DeviceGuard guard(plan->device);
+    SARBP_TRY_CUDA(guard.status);
+    return hypotheses_impl(plan, geometry, num_hypotheses, images, image_memory, flags,
+                           static_cast<cudaStream_t>(stream));
 }
 
 int sarbp_backproject_adjoint(sarbp_plan *plan, const sarbp_geometry *geometry, const void *grad_image,

@@ -133,7 +133,9 @@ __global__ void __launch_bounds__(kThreads, 2) bp_mixed_kernel(const BpLaunch L)
     const uint32_t pulse_bytes = static_cast<uint32_t>(wsize) * 16u;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int ty0 = blockIdx.x * kTY, tx0 = blockIdx.y * TX, iz = blockIdx.z;
+    const int hyp = blockIdx.z / L.nz;  // blockIdx.z = hypothesis * nz + z-slice
+    const int ty0 = blockIdx.x * kTY, tx0 = blockIdx.y * TX, iz = blockIdx.z - hyp * L.nz;
+    const long long goff = static_cast<long long>(hyp) * L.np;
     const double cx = L.left + static_cast<double>(tx0 + TX / 2) * L.dx;
     const double cy = L.bottom + static_cast<double>(ty0 + kTY / 2) * L.dy;
     const double cz = L.zlow + static_cast<double>(iz) * L.dz;
@@ -168,7 +170,7 @@ __global__ void __launch_bounds__(kThreads, 2) bp_mixed_kernel(const BpLaunch L)
     __syncthreads();
 
     const int nblocks = (L.np + PB - 1) / PB;
-    if (nblocks > 0) produce_slots<PB>(L, 0, geo, win_addr, bar_base, warp, lane, cx, cy, cz);
+    if (nblocks > 0) produce_slots<PB>(L, 0, geo, win_addr, bar_base, warp, lane, cx, cy, cz, goff);
     __syncthreads();
 
     int last_issued = 0;
@@ -177,7 +179,7 @@ __global__ void __launch_bounds__(kThreads, 2) bp_mixed_kernel(const BpLaunch L)
         const int s = b & 1;
         if (b + 1 < nblocks) {
             produce_slots<PB>(L, b + 1, geo + (s ^ 1) * PB, win_addr + (s ^ 1) * PB * pulse_bytes,
-                              bar_base + 8 * (s ^ 1), warp, lane, cx, cy, cz);
+                              bar_base + 8 * (s ^ 1), warp, lane, cx, cy, cz, goff);
             last_issued = b + 1;
         }
         const bool ok = mbar_wait_bounded(bar_base + 8 * s, (b >> 1) & 1, L.err);
@@ -230,7 +232,7 @@ __global__ void __launch_bounds__(kThreads, 2) bp_mixed_kernel(const BpLaunch L)
         const int row = tx0 + warp + 8 * k;
         const int col = ty0 + 2 * lane;
         if (row >= L.nx || col >= L.ny) continue;
-        const long long o = (static_cast<long long>(iz) * L.nx + row) * L.ny + col;
+        const long long o = ((static_cast<long long>(hyp) * L.nz + iz) * L.nx + row) * L.ny + col;
         if (L.vec_store && col + 1 < L.ny) {
             float4 v = make_float4(acc_re[k][0], acc_im[k][0], acc_re[k][1], acc_im[k][1]);
             float4 *dst = reinterpret_cast<float4 *>(img + o);
@@ -266,7 +268,7 @@ __global__ void __launch_bounds__(kThreads, 2) bp_mixed_kernel(const BpLaunch L)
 template <int MX, int PB>
 cudaError_t launch_mx_pb(const BpLaunch &L, bool checked, size_t smem, cudaStream_t s) {
     constexpr int TX = 8 * MX;
-    const dim3 grid((L.ny + kTY - 1) / kTY, (L.nx + TX - 1) / TX, L.nz);
+    const dim3 grid((L.ny + kTY - 1) / kTY, (L.nx + TX - 1) / TX, L.nz * L.nhyp);
     auto kern = checked ? bp_mixed_kernel<MX, PB, true> : bp_mixed_kernel<MX, PB, false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;

@@ -20,10 +20,12 @@ constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23: adding it rounds to a
 constexpr uint32_t kRoundMagicBits = 0x4B400000u;
 constexpr double kTwoPi = 6.283185307179586476925286766559;
 
-__device__ __forceinline__ PulseGeo make_geo(const BpLaunch &L, int p, double cx, double cy, double cz) {
+__device__ __forceinline__ PulseGeo make_geo(const BpLaunch &L, int p, long long goff, double cx, double cy,
+                                             double cz) {
     PulseGeo g;
     g.flags = 0;
-    const double ax = L.ax[p], ay = L.ay[p], az = L.az[p], r0 = L.r0[p], f0 = L.f0[p];
+    const long long gi = goff + p;  // geometry of hypothesis goff / np
+    const double ax = L.ax[gi], ay = L.ay[gi], az = L.az[gi], r0 = L.r0[gi], f0 = L.f0[gi];
     const double vx = ax - cx, vy = ay - cy, vz = az - cz;
     const double rc = sqrt(vx * vx + vy * vy + vz * vz);
     const double inv = 1.0 / rc;
@@ -76,13 +78,14 @@ __device__ __forceinline__ PulseGeo make_geo(const BpLaunch &L, int p, double cx
 // count and issues its bulk copy, or just arrives (inactive / past the end).
 template <int PB>
 __device__ __forceinline__ void produce_slots(const BpLaunch &L, int b, PulseGeo *geo_s, uint32_t win_s,
-                                              uint32_t bar, int warp, int lane, double cx, double cy, double cz) {
+                                              uint32_t bar, int warp, int lane, double cx, double cy, double cz,
+                                              long long goff = 0) {
     if (lane != 0) return;
     for (int q = warp; q < PB; q += kWarps) {
         const int p = b * PB + q;
         PulseGeo g;
         g.flags = 0;
-        if (p < L.np) g = make_geo(L, p, cx, cy, cz);
+        if (p < L.np) g = make_geo(L, p, goff, cx, cy, cz);
         geo_s[q] = g;
         if (g.flags & PG_ACTIVE) {
             const uint32_t bytes = static_cast<uint32_t>(L.wsize) * 16u;

@@ -28,6 +28,7 @@ struct BpLaunch {
     int accumulate;
     int vec_store;          // 16-byte aligned image and even ny
     unsigned *err;
+    int nhyp;               // geometry hypotheses (mixed forward kernel): arrays [nhyp][np], images [nhyp][nz][nx][ny]
 };
 
 // Tile shape of the forward kernels (see bp_mixed.cu).
@@ -80,6 +81,8 @@ struct sarbp_plan {
     void *d_partials; // adjoint per-(tile, pulse) partial gradients (allocated on first use)
     size_t partials_bytes;
     double *d_gout;   // adjoint output staging for host outputs [4][np] (allocated on first use)
+    void *d_hyp;      // host-memory staging for hypothesis batches (allocated on first use)
+    size_t hyp_bytes;
     size_t bytes;     // device bytes held
     cufftHandle fft;
     bool fft_ok;

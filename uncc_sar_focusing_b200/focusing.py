@@ -159,6 +159,33 @@ class Plan:
             np.copyto(out, ikeep.reshape(out.shape))
         return out
 
+    def backproject_hypotheses(self, ant_x, ant_y, ant_z, slant_range, start_freq, out=None, accumulate=False):
+        """Images for H antenna-track hypotheses at once: geometry arrays
+        [H, Np] (hypothesis-major), images [H, nz, nx, ny]
+        (sarbp_backproject_hypotheses)."""
+        H, n = int(ant_x.shape[0]), int(ant_x.shape[1])
+        flat = [v.reshape(-1) for v in (ant_x, ant_y, ant_z, slant_range, start_freq)]
+        ptrs = [_ptr(v, np.float64, H * n) for v in flat]
+        mems = {m for _, m, _ in ptrs}
+        if len(mems) != 1:
+            raise ValueError("geometry arrays must all be host arrays or all CUDA tensors")
+        geo = N.Geometry(ptrs[0][0], ptrs[1][0], ptrs[2][0], ptrs[3][0], ptrs[4][0], n, mems.pop())
+        shape = (H,) + tuple(self.image_shape())
+        if out is None:
+            if geo.memory == N.MEMORY_HOST:
+                out = np.zeros(shape, dtype=np.complex64)
+            else:
+                import torch
+
+                out = torch.zeros(shape, dtype=torch.complex64, device=ant_x.device)
+        ip, imem, ikeep = _ptr(out, np.complex64, int(np.prod(shape)))
+        st = N.lib().sarbp_backproject_hypotheses(self._h, ctypes.byref(geo), H, ip, imem,
+                                                  N.ACCUMULATE if accumulate else 0, _stream(out, ant_x))
+        N.check(st, "sarbp_backproject_hypotheses")
+        if imem == N.MEMORY_HOST and ikeep is not out:
+            np.copyto(out, ikeep.reshape(out.shape))
+        return out
+
     def backproject_adjoint(self, ant_x, ant_y, ant_z, slant_range, start_freq, grad_image, accumulate=False):
         """dL/d(ant_x, ant_y, ant_z) as a [3, Np] array and dL/dR0 [Np] for a
         real loss L whose image gradient is grad_image = dL/dRe + j dL/dIm

@@ -243,3 +243,53 @@ def volumetric_scene(K: int = 512, pulses_per_pass: int = 1024, elevations: Sequ
     return Scene(name="volumetric", phase_history=ph, ant_x=ax, ant_y=ay, ant_z=azz, slant_range=r0,
                  start_freq=np.full(Np, freqs[0]), delta_freq=float(freqs[1] - freqs[0]),
                  nfft=nfft if nfft is not None else 8 * K, grid=grid, targets=tg, amplitudes=amps, seed=seed)
+
+
+def slow_time(num_pulses: int) -> np.ndarray:
+    """Normalised slow time tau in [-1, 1] over the aperture."""
+    return np.linspace(-1.0, 1.0, num_pulses)
+
+
+def cubic_track_error(coeffs: np.ndarray, tau: np.ndarray) -> np.ndarray:
+    """[3, Np] position error sum_n c[axis, n] tau^n, n = 0..3 (c is [3, 4])."""
+    powers = np.stack([tau ** n for n in range(4)])  # [4, Np]
+    return np.asarray(coeffs, dtype=np.float64) @ powers
+
+
+def motion_error_scene(K: int = 512, Np: int = 1024, n: int = 512, spacing: float = 0.08, peak: float = 1.5,
+                       walk_sigma: float = 1e-3, seed: int = 4, snr_db: Optional[float] = 20.0,
+                       n_targets: int = 5, extent: float = 20.0, device: Optional[str] = None) -> Scene:
+    """Autofocus scene: the point-target geometry (9.6 GHz, 600 MHz, 4 deg at
+    10 km, 30 deg elevation) with Np pulses of K samples, where the phase
+    history is synthesised from the TRUE antenna track and the scene carries
+    the MEASURED track (ant_x/y/z) the focuser is given:
+        true = measured + e(tau),  e = cubic in slow time per axis (seeded,
+        max |e| <= peak metres on each axis) + Gaussian random walk
+        (walk_sigma metres per pulse).
+    The true cubic coefficients and the full error are attached as
+    scene.true_cubic [3, 4] and scene.true_error [3, Np]."""
+    rng = np.random.default_rng(seed)
+    tg = np.zeros((n_targets, 3))
+    tg[:, :2] = rng.uniform(-extent / 2.0, extent / 2.0, size=(n_targets, 2))
+    amps = np.ones(n_targets, dtype=np.complex128)
+    fc, bw, radius, el = 9.6e9, 600e6, 10e3, 30.0
+    freqs = np.linspace(fc - bw / 2.0, fc + bw / 2.0, K)
+    ax, ay, az = circular_track(Np, radius, el, 0.0, 4.0)
+    measured = np.stack([ax, ay, az])
+    tau = slow_time(Np)
+    coeffs = rng.uniform(-1.0, 1.0, size=(3, 4))
+    cub = cubic_track_error(coeffs, tau)
+    coeffs = coeffs * (peak / np.abs(cub).max(axis=1, keepdims=True))
+    walk = np.cumsum(rng.normal(0.0, walk_sigma, size=(3, Np)), axis=1)
+    err = cubic_track_error(coeffs, tau) + walk
+    true = measured + err
+    r0 = np.full(Np, radius)
+    ph = synthesize_phase_history(freqs, true.T.copy(), r0, tg, amps, device=device)
+    ph = add_noise(ph, snr_db, rng)
+    w = spacing * (n - 1)
+    sc = Scene(name="motion_error", phase_history=np.ascontiguousarray(ph), ant_x=ax, ant_y=ay, ant_z=az,
+               slant_range=r0, start_freq=np.full(Np, freqs[0]), delta_freq=float(freqs[1] - freqs[0]),
+               nfft=8 * K, grid=Grid(nx=n, ny=n, wx=w, wy=w), targets=tg, amplitudes=amps, seed=seed)
+    sc.true_cubic = coeffs
+    sc.true_error = err
+    return sc
