@@ -57,6 +57,8 @@ def parse_args():
     ap.add_argument("--config", choices=["large", "point_targets"], default="large")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
+    ap.add_argument("--no-autofocus", action="store_true")
+    ap.add_argument("--grid-seconds", type=float, default=20.0, help="bound on the grid-search baseline")
     ap.add_argument("--profile", action="store_true",
                     help="one warm-up and one focus step of the workload, nothing else (for ncu captures)")
     ap.add_argument("--pulses", type=int, default=0, help="use only the first N pulses (profiling)")
@@ -95,7 +97,7 @@ class ClockSampler:
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", gpu_id, f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -240,6 +242,71 @@ def roofline_bound(peaks):
     return bound, 1.0 / t[bound], t
 
 
+def autofocus_section(dev, grid_seconds: float):
+    """Motion-error autofocus on the autofocus configuration (config-1
+    geometry, 1024 pulses x 512 samples, 512^2 image; per-axis seeded cubic
+    track error up to 1.5 m plus a 1 mm/pulse random walk): the gradient
+    pipeline (cubic coefficients, then per-pulse line of sight, then PGA)
+    against the reference's multiresolution grid search restated on the same
+    engine (6 quadratic/cubic coefficients, 5 points each, halving boxes),
+    bounded to grid_seconds.  Seconds-to-focus = time for each method to reach
+    the grid search's final entropy."""
+    import numpy as np
+    import torch
+
+    from uncc_sar_focusing_b200 import autofocus as AF
+    from uncc_sar_focusing_b200 import autograd as A
+    from uncc_sar_focusing_b200 import focusing
+    from uncc_sar_focusing_b200 import scenes as S
+
+    sc = S.motion_error_scene(device=dev)
+    torch.cuda.empty_cache()
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    ax, ay, az, r0, f0 = (d(v) for v in (sc.ant_x, sc.ant_y, sc.ant_z, sc.slant_range, sc.start_freq))
+    with focusing.Plan.for_scene(sc, "mixed") as plan:
+        plan.range_compress(d(sc.phase_history))
+        ent = lambda x, y, z, r=r0: float(A.image_entropy(plan.backproject(x, y, z, r, f0)))  # noqa: E731
+        e_measured = ent(ax, ay, az)
+        e_true = ent(*(d(getattr(sc, a) + sc.true_error[i]) for i, a in enumerate(("ant_x", "ant_y", "ant_z"))))
+        AF.focus_motion_error(plan, ax, ay, az, r0, f0, cubic_iters=5, los_iters=5, pga_iters=1)  # warm-up
+        grad = AF.focus_motion_error(plan, ax, ay, az, r0, f0)
+        motion = AF.CubicMotion(ax, ay, az)
+        grid = AF.grid_search_autofocus(plan, motion, r0, f0, span=1.5, points=5, levels=4, batch=128,
+                                        deadline_s=grid_seconds)
+    e_grid = grid.history[-1]["entropy"] if grid.history else float("nan")
+    t_grad = AF.time_to_entropy(grad["timeline"], e_grid)
+    return {
+        "workload": "autofocus: 9.6 GHz / 600 MHz, 4 deg at 10 km, 30 deg el, 1024 pulses x 512 samples, 512^2 "
+                    "image at 0.08 m, 5 targets, 20 dB SNR; track error per axis = seeded cubic (1.5 m peak) + "
+                    "1 mm/pulse random walk",
+        "entropy_measured_track": e_measured, "entropy_true_track": e_true,
+        "gradient": {"entropy_cubic": grad["entropy_cubic"], "entropy_line_of_sight": grad["entropy_los"],
+                     "entropy_pga": grad["entropy_pga"], "seconds": grad["seconds"],
+                     "stages": "Adam on 12 cubic coefficients (300 it) -> Adam on 1024 per-pulse ranges "
+                               "(200 it) -> PGA; gradients from the adjoint kernel"},
+        "grid_search": {"entropy": e_grid, "seconds": grid.seconds, "images": grid.images_formed,
+                        "levels_done": len(grid.history), "bounded_to_s": grid_seconds},
+        "sec_to_focus": {"target_entropy": e_grid, "gradient_s": t_grad, "grid_search_s": grid.seconds,
+                         "speedup": (grid.seconds / t_grad) if t_grad else None},
+    }
+
+
+def profiled_traffic(config: str):
+    """DRAM bytes per backprojection launch from the committed ncu summary of
+    this workload (profiles/), or None."""
+    if config != "large":
+        return None
+    p = os.path.join(ROOT, "profiles", "bp_mixed_large.md")
+    try:
+        with open(p) as fh:
+            for line in fh:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def measured_hbm():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -307,9 +374,10 @@ def gpu_arm(args):
     props = torch.cuda.get_device_properties(local)
     uuid = str(getattr(props, "uuid", ""))
     gpu_id = uuid if uuid.startswith("GPU-") else (f"GPU-{uuid}" if uuid else str(local))
+    # clocks are sampled from here to the end of the kernel-level timings
+    # (the timed steps alone can be shorter than the sampling period)
     sampler = ClockSampler(gpu_id)
     ms = timed(step, args.steps)
-    clocks = sampler.stop()
     ms = max_over_ranks(ms)
     ms_step = ms / args.steps
     value = world * pp / (ms_step * 1e-3)
@@ -320,6 +388,13 @@ def gpu_arm(args):
     plan.focus(ph_d, *geo_d, out=img_d)
     bp_ms = max_over_ranks(timed(lambda: plan.backproject(*geo_d, out=img_d), reps)) / reps
     plan.check()
+    # a second of back-to-back steps so the clock record covers steady load
+    t_end = time.perf_counter() + 1.0
+    while time.perf_counter() < t_end:
+        for _ in range(20):
+            step()
+        torch.cuda.synchronize()
+    clocks = sampler.stop()
 
     # FP64 GPU path on the same inputs: accuracy reference and the FP64 baseline
     img_mixed = img_d.clone()
@@ -391,6 +466,12 @@ def gpu_arm(args):
                          "t_min_per_pixel_pulse_s": tmin},
             "clocks": clocks,
         }
+        if world == 1 and not args.no_autofocus:
+            line["autofocus"] = autofocus_section(dev, args.grid_seconds)
+        traffic = profiled_traffic(args.config)
+        if traffic is not None:
+            line["roofline"]["traffic"] = traffic
+            line["roofline"]["traffic_source"] = "profiles/bp_mixed_large.md (ncu dram__bytes_read+write, per launch)"
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_reference_rate(sc, args.cpu_seconds)
             cb.pop("seconds", None)
