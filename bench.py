@@ -68,18 +68,18 @@ def parse_args():
 def make_scene(config: str, rank: int, world: int, device):
     from uncc_sar_focusing_b200 import scenes as S
 
+    from uncc_sar_focusing_b200 import sharding as SH
+
     if config == "large":
         sc = S.large_scene(device=device)
         desc = ("large: 1024 samples x 2048 pulses complex64, fc 9.6 GHz / 640 MHz, 30 deg at 8 km, 45 deg el, "
                 "2000 Rayleigh scatterers, 1024x1024 image over 100 m, Nfft 8192")
-        span = 100.0
     else:
         sc = S.point_target_scene(device=device)
         desc = ("point_targets: 424 samples x 512 pulses complex64, fc 9.6 GHz / 600 MHz, 4 deg at 10 km, "
                 "30 deg el, 5 unit targets, 20 dB SNR, 256x256 image at 0.08 m, Nfft 3392")
-        span = sc.grid.wy + sc.grid.wy / (sc.grid.ny - 1)
-    # rank r takes slab r of an N-slab image along y
-    sc.grid.y0 = sc.grid.y0 + (rank - (world - 1) / 2.0) * span
+    # weak scaling: rank r forms slab r of a (world x per-GPU) image along y
+    sc.grid = SH.slab_grid(SH.weak_scaling_grid(sc.grid, world), rank, world)
     return sc, desc
 
 
