@@ -326,12 +326,17 @@ def gpu_arm(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    local = local % max(1, torch.cuda.device_count())
     torch.cuda.set_device(local)
     dev = f"cuda:{local}"
     if world > 1:
         from datetime import timedelta
 
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device(dev))
+        # NCCL for the barrier and the max over ranks; SARBP_BENCH_BACKEND=gloo
+        # runs the multi-rank path with several ranks on one GPU (smoke tests)
+        backend = os.environ.get("SARBP_BENCH_BACKEND", "nccl")
+        kw = {"device_id": torch.device(dev)} if backend == "nccl" else {}
+        dist.init_process_group(backend, timeout=timedelta(seconds=300), **kw)
 
     def barrier():
         if world > 1:
@@ -340,7 +345,7 @@ def gpu_arm(args):
     def max_over_ranks(x: float) -> float:
         if world == 1:
             return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        t = torch.tensor([x], dtype=torch.float64, device=dev if dist.get_backend() == "nccl" else "cpu")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
