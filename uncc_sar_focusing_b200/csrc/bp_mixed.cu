@@ -39,6 +39,12 @@ namespace {
 
 using namespace tile;
 
+// pulses of a common-path stage unrolled together (0: the whole stage)
+#ifndef SARBP_FAST_UNROLL
+#define SARBP_FAST_UNROLL 0
+#endif
+constexpr int kFastUnroll = SARBP_FAST_UNROLL;
+
 
 // One pulse into the thread's MX x 2 pixels.  The two columns l = 0, 1 of a
 // row form a pair and all of their geometry arithmetic runs as paired FP32
@@ -120,8 +126,8 @@ __device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, uint32_t w_a
     }
 }
 
-template <int MX, int PB, bool CHECKED>
-__global__ void __launch_bounds__(kThreads, 2) bp_mixed_kernel(const BpLaunch L) {
+template <int MX, int PB, bool CHECKED, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) bp_mixed_kernel(const BpLaunch L) {
     constexpr int TX = 8 * MX;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
@@ -191,7 +197,8 @@ __global__ void __launch_bounds__(kThreads, 2) bp_mixed_kernel(const BpLaunch L)
             const int all_f = __reduce_and_sync(0xffffffffu, lane < nq ? my_flags : PG_ACTIVE);
             const uint32_t w0 = win_addr + s * PB * pulse_bytes;
             if (nq == PB && (all_f & PG_ACTIVE) && !(any_f & (PG_GATE | PG_NEAR))) {
-#pragma unroll
+                constexpr int kUnroll = kFastUnroll > 0 ? kFastUnroll : PB;
+#pragma unroll kUnroll
                 for (int q = 0; q < PB; ++q)
                     accumulate_pulse<MX, false, false, CHECKED>(geo[s * PB + q], w0 + q * pulse_bytes, zero_addr,
                                                                 i0, j0, lam, nd2, acc_re, acc_im, wsize, L.err);
@@ -269,7 +276,11 @@ template <int MX, int PB>
 cudaError_t launch_mx_pb(const BpLaunch &L, bool checked, size_t smem, cudaStream_t s) {
     constexpr int TX = 8 * MX;
     const dim3 grid((L.ny + kTY - 1) / kTY, (L.nx + TX - 1) / TX, L.nz * L.nhyp);
-    auto kern = checked ? bp_mixed_kernel<MX, PB, true> : bp_mixed_kernel<MX, PB, false>;
+    // two CTAs per SM (128 registers) by default; one CTA per SM (up to 255
+    // registers) when the stage needs more shared memory than two CTAs get
+    const bool one_cta = smem > 113u * 1024u;
+    auto kern = checked ? (one_cta ? bp_mixed_kernel<MX, PB, true, 1> : bp_mixed_kernel<MX, PB, true, 2>)
+                        : (one_cta ? bp_mixed_kernel<MX, PB, false, 1> : bp_mixed_kernel<MX, PB, false, 2>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     kern<<<grid, kThreads, smem, s>>>(L);
