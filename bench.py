@@ -15,7 +15,9 @@ the data path; the ranks only meet for the timing barrier and the max).
 Printed on rank 0 as one JSON line:
   value     pixel-pulses/s over all ranks, inputs resident in HBM
   e2e       the same through the C ABI with pinned host buffers: H2D of the
-            phase history and geometry, D2H of the image, every step
+            phase history and geometry, D2H of the image, every step, through
+            the pipelined sarbp_focus_submit/wait (copies of neighbouring
+            steps overlap the kernels); the synchronous sarbp_focus beside it
   roofline  the backprojection kernel against the pipe that bounds it, with
             per-pixel-pulse algorithmic work 10 FP64 + 16 FP32 flops,
             2 transcendental (MUFU) ops and 16 B of on-chip gather, and the
@@ -423,19 +425,30 @@ def gpu_arm(args):
         h = torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
         h.copy_(v.cpu())
         geo_h.append(h)
-    img_h = torch.empty(img_d.shape, dtype=img_d.dtype, pin_memory=True)
-    ph_n, geo_n, img_n = ph_h.numpy(), [g.numpy() for g in geo_h], img_h.numpy()
-    e2e_step = lambda: plan.focus(ph_n, *geo_n, out=img_n)  # noqa: E731
-    for _ in range(2):
-        e2e_step()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_step()
-    e2e_s = max_over_ranks(time.perf_counter() - t0) / args.steps
+    img_h = [torch.empty(img_d.shape, dtype=img_d.dtype, pin_memory=True) for _ in range(2)]
+    ph_n, geo_n, img_n = ph_h.numpy(), [g.numpy() for g in geo_h], [h.numpy() for h in img_h]
+
+    def e2e_run(n, pipelined):
+        # every step uploads its aperture and downloads its image; pipelined
+        # steps overlap step i's kernels with i+1's upload and i-1's download
+        barrier()
+        t0 = time.perf_counter()
+        for i in range(n):
+            if pipelined:
+                plan.focus_submit(ph_n, *geo_n, out=img_n[i % 2])
+            else:
+                plan.focus(ph_n, *geo_n, out=img_n[i % 2])
+        plan.focus_wait()
+        return max_over_ranks(time.perf_counter() - t0) / n
+
+    e2e_run(3, True)
+    e2e_s = e2e_run(args.steps, True)
+    e2e_sync_s = e2e_run(args.steps, False)
     h2d = ph_n.nbytes + sum(g.nbytes for g in geo_n)
-    d2h = img_n.nbytes
-    assert np.allclose(img_n, img_mixed.cpu().numpy(), rtol=0, atol=1e-6 * float(np.abs(img_n).max()))
+    d2h = img_n[0].nbytes
+    ref = img_mixed.cpu().numpy()
+    for h in img_n:
+        assert np.array_equal(h, ref)
 
     line = None
     if rank == 0:
@@ -459,7 +472,10 @@ def gpu_arm(args):
             "fp64_gpu": {"bp_value": pp / (fp64_ms * 1e-3), "unit": UNIT,
                          "mixed_speedup": (pp / (bp_ms * 1e-3)) / (pp / (fp64_ms * 1e-3))},
             "e2e": {"value": world * pp / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3,
+                    "api": "sarbp_focus_submit/sarbp_focus_wait, pinned host buffers",
+                    "synchronous": {"value": world * pp / e2e_sync_s, "ms_per_step": e2e_sync_s * 1e3,
+                                    "api": "sarbp_focus, pinned host buffers"}},
             "gpu_launches": 3 * args.steps,
             "kernels": {"bp_ms": bp_ms, "range_compress_ms": rc_ms,
                         "range_compress_hbm": {"bytes": rc_bytes, "achieved_gbs": rc_bytes / (rc_ms * 1e-3) / 1e9,

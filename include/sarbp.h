@@ -192,6 +192,28 @@ SARBP_API int sarbp_backproject_adjoint(sarbp_plan *plan, const sarbp_geometry *
                                         int grad_memory, double *grad_ant, double *grad_r0, int out_memory,
                                         int flags, void *stream);
 
+/* Pipelined focusing of a stream of apertures held in HOST memory: the
+ * reference's cuda_focus_SAR_image (cuda_sar_focusing.hpp:526-723) copies in,
+ * computes and copies out one aperture at a time; here submitting aperture
+ * t+1 while aperture t computes overlaps t+1's upload and t-1's download with
+ * t's kernels (plan-owned streams, two staging slots).
+ *
+ * sarbp_focus_submit enqueues range compression + backprojection of one
+ * aperture whose phase history and geometry are host memory into a host
+ * image (complex64 MIXED / complex128 FP64 on the plan's grid) and returns a
+ * ticket (1, 2, ...).  Page-locked (pinned) buffers make the copies
+ * asynchronous; pageable ones still work, without overlap.  The aperture and
+ * image buffers must stay untouched until a wait covering the ticket returns.
+ * With two submissions outstanding a third first waits for the oldest.
+ * sarbp_focus_wait(plan, ticket) waits for every submission up to ticket
+ * (0: all) and returns the first error any of them recorded, once.  The
+ * plan's other calls first wait for outstanding submissions (keeping an
+ * error they recorded for the next sarbp_focus_wait); work the caller queued
+ * on its own streams with device buffers must be complete before a submit. */
+SARBP_API int sarbp_focus_submit(sarbp_plan *plan, const sarbp_aperture *aperture, void *image,
+                                 unsigned long long *ticket);
+SARBP_API int sarbp_focus_wait(sarbp_plan *plan, unsigned long long ticket);
+
 /* One call, no plan kept: create, focus, destroy (host or device buffers). */
 SARBP_API int sarbp_focus_image(const sarbp_plan_desc *desc, const sarbp_aperture *aperture, void *image,
                       int image_memory);

@@ -65,6 +65,8 @@ def test_null_pointers_are_reported():
     assert lib.sarbp_focus(None, None, None, 0, None) == N.SARBP_ERR_NULL_POINTER
     assert lib.sarbp_backproject(None, None, None, 0, 0, None) == N.SARBP_ERR_NULL_POINTER
     assert lib.sarbp_range_compress(None, None, 0, 0, None) == N.SARBP_ERR_NULL_POINTER
+    assert lib.sarbp_focus_submit(None, None, None, None) == N.SARBP_ERR_NULL_POINTER
+    assert lib.sarbp_focus_wait(None, 0) == N.SARBP_ERR_NULL_POINTER
 
 
 def test_no_device_is_a_status_not_a_crash():

@@ -38,7 +38,7 @@ EXPORTED = (
     "sarbp_abi_version", "sarbp_status_string", "sarbp_plan_create", "sarbp_plan_destroy",
     "sarbp_plan_workspace_bytes", "sarbp_range_compress", "sarbp_get_range_profiles", "sarbp_backproject",
     "sarbp_focus", "sarbp_focus_image", "sarbp_plan_check", "sarbp_backproject_noalloc",
-    "sarbp_backproject_adjoint", "sarbp_backproject_hypotheses",
+    "sarbp_backproject_adjoint", "sarbp_backproject_hypotheses", "sarbp_focus_submit", "sarbp_focus_wait",
 )
 
 
@@ -90,6 +90,8 @@ def lib():
         L.sarbp_backproject_noalloc.argtypes = [P(PlanDesc), vp, P(Geometry), vp, i, vp]
         L.sarbp_backproject_adjoint.argtypes = [vp, P(Geometry), vp, i, vp, vp, i, i, vp]
         L.sarbp_backproject_hypotheses.argtypes = [vp, P(Geometry), i, vp, i, i, vp]
+        L.sarbp_focus_submit.argtypes = [vp, P(Aperture), vp, P(ctypes.c_ulonglong)]
+        L.sarbp_focus_wait.argtypes = [vp, ctypes.c_ulonglong]
         for name in EXPORTED:
             if name != "sarbp_status_string":
                 getattr(L, name).restype = i

@@ -33,6 +33,12 @@ int from_cufft(cufftResult r) {
     return SARBP_ERR_CUFFT;
 }
 
+#define SARBP_TRY(call)                       \
+    do {                                      \
+        const int st_ = (call);               \
+        if (st_ != SARBP_OK) return st_;      \
+    } while (0)
+
 #define SARBP_TRY_CUDA(call)                  \
     do {                                      \
         const cudaError_t e_ = (call);        \
@@ -138,8 +144,50 @@ int choose_tile(sarbp_plan *p) {
     return SARBP_ERR_UNSUPPORTED;
 }
 
+}  // namespace
+
+// Pipelined host-buffer focusing: three streams (uploads, kernels, downloads)
+// and kDepth staging slots.  Submission t uses slot t % kDepth; its upload is
+// enqueued only after submission t - kDepth has been collected on the host,
+// which also orders the slot's reuse.  Per-slot error words travel back with
+// the image into page-locked host memory.
+struct sarbp_pipe {
+    static constexpr int kDepth = 2;
+    cudaStream_t in = nullptr, work = nullptr, out = nullptr;
+    cudaEvent_t in_ready[kDepth] = {}, work_done[kDepth] = {}, out_done[kDepth] = {};
+    void *d_ph[kDepth] = {};
+    double *d_geo[kDepth] = {};
+    void *d_img[kDepth] = {};
+    unsigned *d_err = nullptr;  // [kDepth]
+    unsigned *h_err = nullptr;  // [kDepth], page-locked
+    unsigned long long submitted = 0, collected = 0;
+    int pending = SARBP_OK;  // first error of a collected submission, not yet reported
+};
+
+namespace {
+
+void destroy_pipe(sarbp_pipe *q) {
+    if (!q) return;
+    for (cudaStream_t s : {q->in, q->work, q->out})
+        if (s) cudaStreamSynchronize(s);
+    for (int i = 0; i < sarbp_pipe::kDepth; ++i) {
+        for (cudaEvent_t e : {q->in_ready[i], q->work_done[i], q->out_done[i]})
+            if (e) cudaEventDestroy(e);
+        cudaFree(q->d_ph[i]);
+        cudaFree(q->d_geo[i]);
+        cudaFree(q->d_img[i]);
+    }
+    cudaFree(q->d_err);
+    if (q->h_err) cudaFreeHost(q->h_err);
+    for (cudaStream_t s : {q->in, q->work, q->out})
+        if (s) cudaStreamDestroy(s);
+    cudaGetLastError();
+    delete q;
+}
+
 void release(sarbp_plan *p) {
     if (!p) return;
+    destroy_pipe(p->pipe);
     if (p->fft_ok) cufftDestroy(p->fft);
     cudaFree(p->d_ph);
     cudaFree(p->d_geo);
@@ -175,15 +223,19 @@ int check_geometry_host(const sarbp_geometry *g) {
     return SARBP_OK;
 }
 
+int status_from_bits(unsigned bits) {
+    if (bits & ERRBIT_TIMEOUT) return SARBP_ERR_KERNEL_TIMEOUT;
+    if (bits & ERRBIT_NOT_FINITE) return SARBP_ERR_NOT_FINITE;
+    if (bits & ERRBIT_BOUNDS) return SARBP_ERR_KERNEL_BOUNDS;
+    return SARBP_OK;
+}
+
 int read_errors(sarbp_plan *p, cudaStream_t s) {
     SARBP_TRY_CUDA(cudaStreamSynchronize(s));
     unsigned bits = 0;
     SARBP_TRY_CUDA(cudaMemcpy(&bits, p->d_err, sizeof(bits), cudaMemcpyDeviceToHost));
     if (bits) SARBP_TRY_CUDA(cudaMemset(p->d_err, 0, sizeof(unsigned)));
-    if (bits & ERRBIT_TIMEOUT) return SARBP_ERR_KERNEL_TIMEOUT;
-    if (bits & ERRBIT_NOT_FINITE) return SARBP_ERR_NOT_FINITE;
-    if (bits & ERRBIT_BOUNDS) return SARBP_ERR_KERNEL_BOUNDS;
-    return SARBP_OK;
+    return status_from_bits(bits);
 }
 
 int range_compress_impl(sarbp_plan *p, const void *ph, int np, int memory, cudaStream_t s) {
@@ -424,6 +476,129 @@ int adjoint_impl(sarbp_plan *p, const sarbp_geometry *geo, const void *grad, int
     return SARBP_OK;
 }
 
+int create_pipe(sarbp_plan *p) {
+    sarbp_pipe *q = new (std::nothrow) sarbp_pipe();
+    if (!q) return SARBP_ERR_OUT_OF_MEMORY;
+    p->pipe = q;  // release() tears down whatever was created if a step fails
+    for (cudaStream_t *s : {&q->in, &q->work, &q->out})
+        SARBP_TRY_CUDA(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
+    const sarbp_grid &g = p->desc.grid;
+    const size_t npix = static_cast<size_t>(g.nx) * g.ny * g.nz;
+    const size_t np = static_cast<size_t>(p->np_cap);
+    for (int i = 0; i < sarbp_pipe::kDepth; ++i) {
+        for (cudaEvent_t *e : {&q->in_ready[i], &q->work_done[i], &q->out_done[i]})
+            SARBP_TRY_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        int st;
+        if ((st = alloc(p, &q->d_ph[i], np * p->K * 8)) ||
+            (st = alloc(p, reinterpret_cast<void **>(&q->d_geo[i]), 5 * np * sizeof(double))) ||
+            (st = alloc(p, &q->d_img[i], npix * cplx_bytes(p))))
+            return st;
+    }
+    const int st = alloc(p, reinterpret_cast<void **>(&q->d_err), sarbp_pipe::kDepth * sizeof(unsigned));
+    if (st != SARBP_OK) return st;
+    SARBP_TRY_CUDA(cudaMemset(q->d_err, 0, sarbp_pipe::kDepth * sizeof(unsigned)));
+    SARBP_TRY_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&q->h_err), sarbp_pipe::kDepth * sizeof(unsigned),
+                                 cudaHostAllocDefault));
+    return SARBP_OK;
+}
+
+// Wait on the host for submission t (the oldest not yet collected) and keep
+// the first error it recorded.
+int collect_one(sarbp_pipe *q) {
+    const unsigned long long t = q->collected + 1;
+    const int slot = static_cast<int>(t % sarbp_pipe::kDepth);
+    SARBP_TRY_CUDA(cudaEventSynchronize(q->out_done[slot]));
+    const int st = status_from_bits(q->h_err[slot]);
+    if (q->pending == SARBP_OK) q->pending = st;
+    q->collected = t;
+    return SARBP_OK;
+}
+
+int drain_pipe(sarbp_plan *p) {
+    sarbp_pipe *q = p->pipe;
+    if (!q) return SARBP_OK;
+    while (q->collected < q->submitted) {
+        const int st = collect_one(q);
+        if (st != SARBP_OK) return st;
+    }
+    return SARBP_OK;
+}
+
+int focus_submit_impl(sarbp_plan *p, const sarbp_aperture *ap, void *image, unsigned long long *ticket) {
+    if (!ap || !image || !ticket) return SARBP_ERR_NULL_POINTER;
+    const sarbp_geometry *geo = &ap->geometry;
+    if (!ap->phase_history || !geo->ant_x || !geo->ant_y || !geo->ant_z || !geo->slant_range || !geo->start_freq)
+        return SARBP_ERR_NULL_POINTER;
+    const int np = geo->num_pulses;
+    if (np < 1 || np > p->np_cap || ap->phase_history_memory != SARBP_MEMORY_HOST ||
+        geo->memory != SARBP_MEMORY_HOST)
+        return SARBP_ERR_INVALID_ARGUMENT;
+    int st = check_geometry_host(geo);
+    if (st != SARBP_OK) return st;
+    if (!p->pipe && (st = create_pipe(p)) != SARBP_OK) {
+        destroy_pipe(p->pipe);
+        p->pipe = nullptr;
+        return st;
+    }
+    sarbp_pipe *q = p->pipe;
+    const unsigned long long t = q->submitted + 1;
+    const int slot = static_cast<int>(t % sarbp_pipe::kDepth);
+    // the slot's previous user (t - kDepth) must have left the device: after
+    // this, its upload, kernels and download have all completed
+    while (q->collected + sarbp_pipe::kDepth < t)
+        if ((st = collect_one(q)) != SARBP_OK) return st;
+
+    // uploads
+    SARBP_TRY_CUDA(cudaMemcpyAsync(q->d_ph[slot], ap->phase_history, static_cast<size_t>(np) * p->K * 8,
+                                   cudaMemcpyHostToDevice, q->in));
+    const double *src[5] = {geo->ant_x, geo->ant_y, geo->ant_z, geo->slant_range, geo->start_freq};
+    const double *dg[5];
+    for (int i = 0; i < 5; ++i) {
+        double *d = q->d_geo[slot] + static_cast<size_t>(i) * p->np_cap;
+        SARBP_TRY_CUDA(cudaMemcpyAsync(d, src[i], sizeof(double) * np, cudaMemcpyHostToDevice, q->in));
+        dg[i] = d;
+    }
+    SARBP_TRY_CUDA(cudaEventRecord(q->in_ready[slot], q->in));
+
+    // kernels: range compression into the plan's rows, then backprojection
+    SARBP_TRY_CUDA(cudaStreamWaitEvent(q->work, q->in_ready[slot], 0));
+    st = range_compress_impl(p, q->d_ph[slot], np, SARBP_MEMORY_DEVICE, q->work);
+    if (st != SARBP_OK) return st;
+    BpLaunch L = launch_params(p, dg[0], dg[1], dg[2], dg[3], dg[4], np, q->d_img[slot], 0);
+    L.err = q->d_err + slot;
+    SARBP_TRY_CUDA(p->precision == SARBP_PRECISION_FP64 ? launch_bp_fp64(L, p->tile, p->smem, q->work)
+                                                         : launch_bp_mixed(L, p->tile, false, p->smem, q->work));
+    SARBP_TRY_CUDA(cudaEventRecord(q->work_done[slot], q->work));
+
+    // downloads: the image, then the slot's error word (cleared for reuse)
+    const sarbp_grid &g = p->desc.grid;
+    const size_t img_bytes = static_cast<size_t>(g.nx) * g.ny * g.nz * cplx_bytes(p);
+    SARBP_TRY_CUDA(cudaStreamWaitEvent(q->out, q->work_done[slot], 0));
+    SARBP_TRY_CUDA(cudaMemcpyAsync(image, q->d_img[slot], img_bytes, cudaMemcpyDeviceToHost, q->out));
+    SARBP_TRY_CUDA(cudaMemcpyAsync(q->h_err + slot, q->d_err + slot, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                   q->out));
+    SARBP_TRY_CUDA(cudaMemsetAsync(q->d_err + slot, 0, sizeof(unsigned), q->out));
+    SARBP_TRY_CUDA(cudaEventRecord(q->out_done[slot], q->out));
+    q->submitted = t;
+    *ticket = t;
+    return SARBP_OK;
+}
+
+int focus_wait_impl(sarbp_plan *p, unsigned long long ticket) {
+    sarbp_pipe *q = p->pipe;
+    const unsigned long long last = q ? q->submitted : 0;
+    if (ticket == 0) ticket = last;
+    if (ticket > last) return SARBP_ERR_INVALID_ARGUMENT;
+    while (q && q->collected < ticket) {
+        const int st = collect_one(q);
+        if (st != SARBP_OK) return st;
+    }
+    if (!q) return SARBP_OK;
+    const int st = q->pending;
+    q->pending = SARBP_OK;
+    return st;
+}
+
 }  // namespace
 
 extern "C" {
@@ -568,6 +743,7 @@ int sarbp_range_compress(sarbp_plan *plan, const void *phase_history, int num_pu
     if (!plan) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
+    SARBP_TRY(drain_pipe(plan));
     return range_compress_impl(plan, phase_history, num_pulses, memory, static_cast<cudaStream_t>(stream));
 }
 
@@ -577,6 +753,7 @@ int sarbp_get_range_profiles(sarbp_plan *plan, void *out, int memory, void *stre
     if (plan->np_ready < 1) return SARBP_ERR_INVALID_ARGUMENT;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
+    SARBP_TRY(drain_pipe(plan));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t bytes = static_cast<size_t>(plan->np_ready) * plan->nfft * cplx_bytes(plan);
     SARBP_TRY_CUDA(cudaMemcpyAsync(out, plan->d_fft, bytes,
@@ -591,6 +768,7 @@ int sarbp_backproject(sarbp_plan *plan, const sarbp_geometry *geometry, void *im
     if (!plan) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
+    SARBP_TRY(drain_pipe(plan));
     return backproject_impl(plan, geometry, image, image_memory, flags, static_cast<cudaStream_t>(stream));
 }
 
@@ -598,6 +776,7 @@ int sarbp_focus(sarbp_plan *plan, const sarbp_aperture *ap, void *image, int ima
     if (!plan || !ap) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
+    SARBP_TRY(drain_pipe(plan));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int st = range_compress_impl(plan, ap->phase_history, ap->geometry.num_pulses, ap->phase_history_memory, s);
     if (st != SARBP_OK) return st;
@@ -620,6 +799,7 @@ int sarbp_backproject_hypotheses(sarbp_plan *plan, const sarbp_geometry *geometr
     if (!plan) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
+    SARBP_TRY(drain_pipe(plan));
     return hypotheses_impl(plan, geometry, num_hypotheses, images, image_memory, flags,
                            static_cast<cudaStream_t>(stream));
 }
@@ -630,8 +810,23 @@ int sarbp_backproject_adjoint(sarbp_plan *plan, const sarbp_geometry *geometry, 
     if (!plan) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
+    SARBP_TRY(drain_pipe(plan));
     return adjoint_impl(plan, geometry, grad_image, grad_memory, grad_ant, grad_r0, out_memory, flags,
                         static_cast<cudaStream_t>(stream));
+}
+
+int sarbp_focus_submit(sarbp_plan *plan, const sarbp_aperture *aperture, void *image, unsigned long long *ticket) {
+    if (!plan) return SARBP_ERR_NULL_POINTER;
+    DeviceGuard guard(plan->device);
+    SARBP_TRY_CUDA(guard.status);
+    return focus_submit_impl(plan, aperture, image, ticket);
+}
+
+int sarbp_focus_wait(sarbp_plan *plan, unsigned long long ticket) {
+    if (!plan) return SARBP_ERR_NULL_POINTER;
+    DeviceGuard guard(plan->device);
+    SARBP_TRY_CUDA(guard.status);
+    return focus_wait_impl(plan, ticket);
 }
 
 int sarbp_plan_check(sarbp_plan *plan, void *stream) {

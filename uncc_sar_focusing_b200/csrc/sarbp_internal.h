@@ -87,4 +87,5 @@ struct sarbp_plan {
     cufftHandle fft;
     bool fft_ok;
     int np_ready;     // pulses in the current range profiles
+    struct sarbp_pipe *pipe;  // pipelined host-buffer focusing (created on first submit)
 };

@@ -224,6 +224,49 @@ class Plan:
             np.copyto(out, ikeep.reshape(out.shape))
         return out
 
+    # -- pipelined host-buffer focusing ---------------------------------------
+    def focus_submit(self, phase_history, ant_x, ant_y, ant_z, slant_range, start_freq, out) -> int:
+        """Queue range compression + backprojection of a host aperture into
+        the host image `out` and return its ticket (sarbp_focus_submit).
+        Upload, kernels and download of successive submissions overlap when
+        the arrays are page-locked (e.g. numpy views of pinned torch tensors).
+        Neither the inputs nor `out` may be touched until `focus_wait` covers
+        the ticket; `out` must be a C-contiguous array of the plan's image
+        dtype and shape, written in place."""
+        if _is_torch(out) or not isinstance(out, np.ndarray) or out.dtype != self.image_dtype \
+                or not out.flags.c_contiguous or out.size != int(np.prod(self.image_shape())):
+            raise ValueError(f"out must be a C-contiguous {np.dtype(self.image_dtype)} numpy array "
+                             f"of shape {self.image_shape()}")
+        geo, keep = self._geometry(ant_x, ant_y, ant_z, slant_range, start_freq)
+        if geo.memory != N.MEMORY_HOST:
+            raise ValueError("focus_submit takes host (numpy) geometry arrays")
+        if int(phase_history.shape[0]) != geo.num_pulses:
+            raise ValueError("phase history and geometry disagree on the pulse count")
+        pp, pmem, pkeep = _ptr(phase_history, np.complex64, geo.num_pulses * self.K)
+        if pmem != N.MEMORY_HOST:
+            raise ValueError("focus_submit takes a host (numpy) phase history")
+        ap = N.Aperture(pp, pmem, geo)
+        t = ctypes.c_ulonglong()
+        st = N.lib().sarbp_focus_submit(self._h, ctypes.byref(ap), ctypes.c_void_p(out.ctypes.data),
+                                        ctypes.byref(t))
+        N.check(st, "sarbp_focus_submit")
+        inflight = self.__dict__.setdefault("_inflight", {})
+        inflight[t.value] = (keep, pkeep, out)
+        # the library collected everything older than its two staging slots
+        for old in [k for k in inflight if k + 2 <= t.value]:
+            inflight.pop(old)
+        self.num_pulses_ready = geo.num_pulses
+        return t.value
+
+    def focus_wait(self, ticket: int = 0) -> None:
+        """Wait for every submission up to `ticket` (0: all) and raise the
+        first error one of them recorded (sarbp_focus_wait)."""
+        st = N.lib().sarbp_focus_wait(self._h, ctypes.c_ulonglong(int(ticket)))
+        inflight = self.__dict__.get("_inflight", {})
+        for old in [k for k in inflight if ticket == 0 or k <= ticket]:
+            inflight.pop(old)
+        N.check(st, "sarbp_focus_wait")
+
     def check(self) -> None:
         """Synchronise and raise if a kernel recorded an error."""
         import torch
