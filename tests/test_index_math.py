@@ -102,3 +102,109 @@ def test_swath_edge_and_odd_grid_indices():
 def test_near_field_indices():
     sc = S.point_target_scene(K=64, Np=32, n=64, spacing=0.1, nfft=512, snr_db=None, n_targets=1, radius=60.0)
     check_scene(sc, 4)
+
+
+# ---- work split of the forward kernels (tile::sk_lo / sk_owner / sk_slot) ----
+
+def sk_lo(c, units, G):
+    return c * units // G
+
+
+def sk_owner(u, units, G):
+    c = u * G // units
+    while c + 1 < G and sk_lo(c + 1, units, G) <= u:
+        c += 1
+    while c > 0 and sk_lo(c, units, G) > u:
+        c -= 1
+    return c
+
+
+def simulate_split(tiles, stages, G):
+    """Replay the kernels' unit loop: which (tile, stage range) each CTA
+    accumulates, where it flushes, and what the fix-up kernel reads."""
+    units = tiles * stages
+    covered = np.zeros(units, dtype=np.int64)
+    stored_whole = {}
+    slot_writes = {}
+    for c in range(G):
+        lo, hi = sk_lo(c, units, G), sk_lo(c + 1, units, G)
+        n = hi - lo
+        seg, seg_first, seg_units = 0, lo % stages, []
+        for i in range(n):
+            u = lo + i
+            t, b = divmod(u, stages)
+            covered[u] += 1
+            seg_units.append(u)
+            if i + 1 == n or (u + 1) // stages != t:
+                if seg_first == 0 and b == stages - 1:
+                    assert t not in stored_whole
+                    stored_whole[t] = c
+                else:
+                    slot = 2 * c + (1 if seg > 0 else 0)
+                    assert slot not in slot_writes, "two segments share a partial slot"
+                    slot_writes[slot] = (t, tuple(seg_units))
+                seg += 1
+                seg_first = 0
+                seg_units = []
+    assert (covered == 1).all()
+    # fix-up: tiles on several CTAs sum the slots of their CTAs
+    for t in range(tiles):
+        c0, c1 = sk_owner(t * stages, units, G), sk_owner(t * stages + stages - 1, units, G)
+        if c0 == c1:
+            assert stored_whole.get(t) == c0
+            continue
+        assert t not in stored_whole
+        got = []
+        for c in range(c0, c1 + 1):
+            slot = 2 * c if sk_lo(c, units, G) >= t * stages else 2 * c + 1
+            tt, us = slot_writes.pop(slot)
+            assert tt == t
+            got.extend(us)
+        assert got == list(range(t * stages, (t + 1) * stages)), "fix-up must add every stage once, in order"
+    assert not slot_writes, "a partial slot nobody reads"
+
+
+@pytest.mark.parametrize("tiles,stages,G", [
+    (512, 256, 296), (512, 256, 148), (32, 64, 296), (1, 7, 5), (7, 1, 3), (1024, 256, 296),
+    (8192, 128, 296), (3, 3, 9), (17, 5, 17), (296, 10, 296), (512, 256, 512),
+])
+def test_work_split_covers_every_unit_once(tiles, stages, G):
+    simulate_split(tiles, stages, min(G, tiles * stages))
+
+
+def test_work_split_random_shapes():
+    rng = np.random.default_rng(5)
+    for _ in range(200):
+        tiles, stages = int(rng.integers(1, 60)), int(rng.integers(1, 40))
+        G = int(rng.integers(1, tiles * stages + 1))
+        simulate_split(tiles, stages, G)
+
+
+def test_unit_cursor_matches_division():
+    """tile::UnitCursor.advance (carry chain b -> ty -> tx -> iz -> hyp) walks
+    units in the same order as the division-based decomposition of u."""
+    for tiles_y, tiles_x, nz, nhyp, stages in [(16, 32, 1, 1, 256), (3, 2, 4, 5, 7), (1, 1, 1, 3, 1), (5, 1, 2, 1, 3)]:
+        units = tiles_y * tiles_x * nz * nhyp * stages
+
+        def decompose(u):
+            t, b = divmod(u, stages)
+            r, ty = divmod(t, tiles_y)
+            q, tx = divmod(r, tiles_x)
+            hyp, iz = divmod(q, nz)
+            return [b, ty, tx, iz, hyp]
+
+        for start in sorted({0, 1, units // 3, units - 2, units - 1}):
+            cur = decompose(start)
+            for u in range(start, min(units, start + 3 * stages + 5)):
+                assert cur == decompose(u)
+                b, ty, tx, iz, hyp = cur
+                b += 1
+                if b == stages:
+                    b, ty = 0, ty + 1
+                    if ty == tiles_y:
+                        ty, tx = 0, tx + 1
+                        if tx == tiles_x:
+                            tx, iz = 0, iz + 1
+                            if iz == nz:
+                                iz, hyp = 0, hyp + 1
+                cur = [b, ty, tx, iz, hyp]

@@ -199,6 +199,7 @@ void release(sarbp_plan *p) {
     cudaFree(p->d_partials);
     cudaFree(p->d_gout);
     cudaFree(p->d_hyp);
+    cudaFree(p->d_sk);
     delete p;
 }
 
@@ -297,6 +298,9 @@ BpLaunch launch_params(const sarbp_plan *p, const double *ax, const double *ay, 
     L.vec_store = ((reinterpret_cast<uintptr_t>(img) & 15u) == 0 && (g.ny % 2) == 0) ? 1 : 0;
     L.err = p->d_err;
     L.nhyp = 1;
+    L.sk_partial = p->d_sk;
+    L.sk_slot_bytes = static_cast<long long>(p->sk_bytes);
+    L.sk_resident = p->sk_resident;
     return L;
 }
 
@@ -678,6 +682,18 @@ int sarbp_plan_create(const sarbp_plan_desc *desc, sarbp_plan **out) {
         (st = alloc(p, reinterpret_cast<void **>(&p->d_err), sizeof(unsigned)))) {
         release(p);
         return st;
+    }
+    // partial-sum slots for launches split over the resident CTAs (two tiles
+    // per CTA); without them every launch runs one CTA per tile
+    p->sk_resident = p->precision == SARBP_PRECISION_FP64 ? bp_fp64_resident(p->tile, p->smem)
+                                                          : bp_mixed_resident(p->tile, p->smem);
+    if (p->sk_resident > 0) {
+        const size_t sk = 2 * static_cast<size_t>(p->sk_resident) * (8 * p->tile.mx) * 64 * cb;
+        if (alloc(p, &p->d_sk, sk) == SARBP_OK) {
+            p->sk_bytes = sk;
+        } else {
+            p->sk_resident = 0;
+        }
     }
     if (cudaMemset(p->d_pairs, 0, np * static_cast<size_t>(p->row_stride) * entry) != cudaSuccess ||
         cudaMemset(p->d_fft, 0, np * p->nfft * cb) != cudaSuccess ||

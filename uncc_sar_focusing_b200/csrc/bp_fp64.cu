@@ -10,6 +10,7 @@
 #include <cstdint>
 
 #include "bp_common.cuh"
+#include "bp_tile.cuh"
 #include "sarbp_internal.h"
 
 namespace sarbp {
@@ -65,6 +66,36 @@ __device__ __forceinline__ void produce_slots64(const BpLaunch &L, int b, PulseG
     }
 }
 
+// Store (or add) a thread's MX x 2 pixels of the tile at (tx0, ty0, z-slice iz).
+template <int MX>
+__device__ __forceinline__ void store_pixels64(const BpLaunch &L, int tx0, int ty0, int iz, int warp, int lane,
+                                               const double (&re)[MX][2], const double (&im)[MX][2]) {
+    double2 *img = static_cast<double2 *>(L.img);
+#pragma unroll
+    for (int k = 0; k < MX; ++k) {
+        const int row = tx0 + warp + 8 * k;
+        if (row >= L.nx) continue;
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            const int col = ty0 + 2 * lane + l;
+            if (col >= L.ny) continue;
+            const long long o = (static_cast<long long>(iz) * L.nx + row) * L.ny + col;
+            double2 v = make_double2(re[k][l], im[k][l]);
+            if (L.accumulate) {
+                const double2 old = img[o];
+                v.x += old.x;
+                v.y += old.y;
+            }
+            img[o] = v;
+        }
+    }
+}
+
+// Tile-local index of pixel (row warp + 8k, column 2 lane + l) in a
+// partial-sum slot of TX x 64 complex128 values.
+__device__ __forceinline__ int slot_pixel(int warp, int lane, int k, int l) { return (warp + 8 * k) * kTY + 2 * lane + l; }
+
+// Units of (tile, stage) split over the CTAs as in bp_mixed.cu (tile::sk_lo).
 template <int MX, int PB>
 __global__ void __launch_bounds__(kThreads, 1) bp_fp64_kernel(const BpLaunch L) {
     constexpr int TX = 8 * MX;
@@ -75,24 +106,21 @@ __global__ void __launch_bounds__(kThreads, 1) bp_fp64_kernel(const BpLaunch L) 
     const int wsize = L.wsize;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int ty0 = blockIdx.x * kTY, tx0 = blockIdx.y * TX, iz = blockIdx.z;
-    const double cx = L.left + static_cast<double>(tx0 + TX / 2) * L.dx;
-    const double cy = L.bottom + static_cast<double>(ty0 + kTY / 2) * L.dy;
-    const double z = L.zlow + static_cast<double>(iz) * L.dz;
-    const double cz = z;
+    const tile::TileGrid tg = tile::tile_grid(L, TX, PB);
+    const long long G = gridDim.x;
+    const long long lo = tile::sk_lo(blockIdx.x, tg.units, G);
+    const int n = static_cast<int>(tile::sk_lo(blockIdx.x + 1, tg.units, G) - lo);
+    if (n <= 0) return;
+    const int S = tg.stages;
 
-    double xs[MX], ys[2], acc_re[MX][2], acc_im[MX][2];
+    double xs[MX], ys[2], z = 0.0, acc_re[MX][2], acc_im[MX][2];
 #pragma unroll
-    for (int k = 0; k < MX; ++k) {
-        xs[k] = L.left + static_cast<double>(tx0 + warp + 8 * k) * L.dx;
+    for (int k = 0; k < MX; ++k)
 #pragma unroll
         for (int l = 0; l < 2; ++l) acc_re[k][l] = acc_im[k][l] = 0.0;
-    }
-#pragma unroll
-    for (int l = 0; l < 2; ++l) ys[l] = L.bottom + static_cast<double>(ty0 + 2 * lane + l) * L.dy;
     const double top = static_cast<double>(L.nfft - 1);
 
-    const uint32_t bar_base = smem_addr(&bars[0]);  // stage s barrier at bar_base + 8*s
+    const uint32_t bar_base = smem_addr(&bars[0]);  // buffer s barrier at bar_base + 8*s
     if (threadIdx.x == 0) {
         mbar_init(bar_base, PB);
         mbar_init(bar_base + 8, PB);
@@ -100,20 +128,43 @@ __global__ void __launch_bounds__(kThreads, 1) bp_fp64_kernel(const BpLaunch L) 
     }
     __syncthreads();
 
-    const int nblocks = (L.np + PB - 1) / PB;
-    if (nblocks > 0) produce_slots64<PB>(L, 0, geo, smem_addr(win), bar_base, warp, lane, cx, cy, cz);
+    auto produce = [&](const tile::UnitCursor &pc, int s) {
+        if (lane != 0) return;
+        const double cx = L.left + static_cast<double>(pc.tx * TX + TX / 2) * L.dx;
+        const double cy = L.bottom + static_cast<double>(pc.ty * kTY + kTY / 2) * L.dy;
+        const double cz = L.zlow + static_cast<double>(pc.iz) * L.dz;
+        produce_slots64<PB>(L, pc.b, geo + s * PB, smem_addr(win + s * PB * wsize), bar_base + 8 * s, warp, lane, cx,
+                            cy, cz);
+    };
+
+    tile::UnitCursor cc, pc;  // consumer at unit i, producer at unit i + 1
+    cc.init(tg, L, lo);
+    pc = cc;
+    produce(pc, 0);
     __syncthreads();
 
     int last_issued = 0;
-    bool timed_out = false;
-    for (int b = 0; b < nblocks; ++b) {
-        const int s = b & 1;
-        if (b + 1 < nblocks) {
-            produce_slots64<PB>(L, b + 1, geo + (s ^ 1) * PB, smem_addr(win + (s ^ 1) * PB * wsize),
-                                bar_base + 8 * (s ^ 1), warp, lane, cx, cy, cz);
-            last_issued = b + 1;
+    int seg = 0;
+    int seg_first = cc.b;
+    bool new_tile = true;
+    for (int i = 0; i < n; ++i) {
+        const int s = i & 1;
+        if (i + 1 < n) {
+            pc.advance(tg, L);
+            produce(pc, s ^ 1);
+            last_issued = i + 1;
         }
-        const bool ok = mbar_wait_bounded(bar_base + 8 * s, (b >> 1) & 1, L.err);
+        const int b = cc.b;
+        if (new_tile) {
+            const int tx0 = cc.tx * TX, ty0 = cc.ty * kTY;
+#pragma unroll
+            for (int k = 0; k < MX; ++k) xs[k] = L.left + static_cast<double>(tx0 + warp + 8 * k) * L.dx;
+#pragma unroll
+            for (int l = 0; l < 2; ++l) ys[l] = L.bottom + static_cast<double>(ty0 + 2 * lane + l) * L.dy;
+            z = L.zlow + static_cast<double>(cc.iz) * L.dz;
+            new_tile = false;
+        }
+        const bool ok = mbar_wait_bounded(bar_base + 8 * s, (i >> 1) & 1, L.err);
         if (ok) {
             const int nq = min(PB, L.np - b * PB);
             for (int q = 0; q < nq; ++q) {
@@ -152,45 +203,99 @@ __global__ void __launch_bounds__(kThreads, 1) bp_fp64_kernel(const BpLaunch L) 
             }
         }
         if (__syncthreads_or(!ok)) {
-            timed_out = true;
-            break;
+            if (threadIdx.x == 0 && last_issued > i)
+                mbar_wait_bounded(bar_base + 8 * (last_issued & 1), (last_issued >> 1) & 1, L.err);
+            return;
         }
-    }
-    if (timed_out) {
-        if (threadIdx.x == 0 && last_issued > 0) mbar_wait_bounded(bar_base + 8 * (last_issued & 1), (last_issued >> 1) & 1, L.err);
-        return;
-    }
-
-    double2 *img = static_cast<double2 *>(L.img);
+        if (i + 1 == n || b == S - 1) {
+            if (seg_first == 0 && b == S - 1) {
+                store_pixels64<MX>(L, cc.tx * TX, cc.ty * kTY, cc.iz, warp, lane, acc_re, acc_im);
+            } else {
+                double2 *slot = static_cast<double2 *>(L.sk_partial) +
+                                (2 * static_cast<long long>(blockIdx.x) + (seg > 0 ? 1 : 0)) * (TX * kTY);
 #pragma unroll
-    for (int k = 0; k < MX; ++k) {
-        const int row = tx0 + warp + 8 * k;
-        if (row >= L.nx) continue;
+                for (int k = 0; k < MX; ++k)
 #pragma unroll
-        for (int l = 0; l < 2; ++l) {
-            const int col = ty0 + 2 * lane + l;
-            if (col >= L.ny) continue;
-            const long long o = (static_cast<long long>(iz) * L.nx + row) * L.ny + col;
-            double2 v = make_double2(acc_re[k][l], acc_im[k][l]);
-            if (L.accumulate) {
-                const double2 old = img[o];
-                v.x += old.x;
-                v.y += old.y;
+                    for (int l = 0; l < 2; ++l)
+                        slot[slot_pixel(warp, lane, k, l)] = make_double2(acc_re[k][l], acc_im[k][l]);
             }
-            img[o] = v;
+#pragma unroll
+            for (int k = 0; k < MX; ++k)
+#pragma unroll
+                for (int l = 0; l < 2; ++l) acc_re[k][l] = acc_im[k][l] = 0.0;
+            ++seg;
+            seg_first = 0;
+            new_tile = true;
         }
+        cc.advance(tg, L);
     }
+}
+
+template <int MX>
+__global__ void __launch_bounds__(kThreads) bp_sk_fixup64_kernel(const BpLaunch L, long long G, int PB) {
+    constexpr int TX = 8 * MX;
+    const tile::TileGrid tg = tile::tile_grid(L, TX, PB);
+    const long long t = blockIdx.x;
+    const long long c0 = tile::sk_owner(t * tg.stages, tg.units, G);
+    const long long c1 = tile::sk_owner(t * tg.stages + tg.stages - 1, tg.units, G);
+    if (c0 == c1) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double re[MX][2], im[MX][2];
+#pragma unroll
+    for (int k = 0; k < MX; ++k)
+#pragma unroll
+        for (int l = 0; l < 2; ++l) re[k][l] = im[k][l] = 0.0;
+    const double2 *part = static_cast<const double2 *>(L.sk_partial);
+    for (long long c = c0; c <= c1; ++c) {
+        const double2 *slot = part + tile::sk_slot(c, t, tg, G) * (TX * kTY);
+#pragma unroll
+        for (int k = 0; k < MX; ++k)
+#pragma unroll
+            for (int l = 0; l < 2; ++l) {
+                const double2 v = slot[slot_pixel(warp, lane, k, l)];
+                re[k][l] += v.x;
+                im[k][l] += v.y;
+            }
+    }
+    int tx0, ty0, iz;
+    tile::tile_origin(tg, t, TX, tx0, ty0, iz);
+    store_pixels64<MX>(L, tx0, ty0, iz, warp, lane, re, im);
 }
 
 template <int MX, int PB>
 cudaError_t launch64(const BpLaunch &L, size_t smem, cudaStream_t s) {
     constexpr int TX = 8 * MX;
-    const dim3 grid((L.ny + kTY - 1) / kTY, (L.nx + TX - 1) / TX, L.nz);
     auto kern = bp_fp64_kernel<MX, PB>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    kern<<<grid, kThreads, smem, s>>>(L);
+    const tile::TileGrid tg = tile::tile_grid(L, TX, PB);
+    if (tg.units < 1) return cudaSuccess;
+    long long G = tg.tiles;
+    if (L.sk_partial && L.sk_resident > 0 && tg.tiles % L.sk_resident != 0) {
+        const long long g = L.sk_resident < tg.units ? L.sk_resident : tg.units;
+        if (2 * g * TX * kTY * static_cast<long long>(sizeof(double2)) <= L.sk_slot_bytes) G = g;
+    }
+    if (G > 0x7fffffffLL) return cudaErrorInvalidValue;
+    kern<<<static_cast<unsigned>(G), kThreads, smem, s>>>(L);
+    e = cudaGetLastError();
+    if (e != cudaSuccess || G == tg.tiles) return e;
+    bp_sk_fixup64_kernel<MX><<<static_cast<unsigned>(tg.tiles), kThreads, 0, s>>>(L, G, PB);
     return cudaGetLastError();
+}
+
+template <int MX, int PB>
+int resident64(size_t smem) {
+    auto kern = bp_fp64_kernel<MX, PB>;
+    int dev = 0, sms = 0, occ = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return occ * sms;
 }
 
 }  // namespace
@@ -198,6 +303,28 @@ cudaError_t launch64(const BpLaunch &L, size_t smem, cudaStream_t s) {
 size_t bp_fp64_smem_bytes(const TileConfig &tc, int wsize) {
     return 32 + 2 * static_cast<size_t>(tc.pb) * sizeof(PulseGeo64) +
            2 * static_cast<size_t>(tc.pb) * static_cast<size_t>(wsize) * 32;
+}
+
+int bp_fp64_resident(const TileConfig &tc, size_t smem) {
+#define SARBP_FP64_CASE(MX_, PB_) \
+    if (tc.mx == MX_ && tc.pb == PB_) return resident64<MX_, PB_>(smem);
+    SARBP_FP64_CASE(4, 16)
+    SARBP_FP64_CASE(4, 8)
+    SARBP_FP64_CASE(4, 4)
+    SARBP_FP64_CASE(4, 2)
+    SARBP_FP64_CASE(4, 1)
+    SARBP_FP64_CASE(2, 16)
+    SARBP_FP64_CASE(2, 8)
+    SARBP_FP64_CASE(2, 4)
+    SARBP_FP64_CASE(2, 2)
+    SARBP_FP64_CASE(2, 1)
+    SARBP_FP64_CASE(1, 16)
+    SARBP_FP64_CASE(1, 8)
+    SARBP_FP64_CASE(1, 4)
+    SARBP_FP64_CASE(1, 2)
+    SARBP_FP64_CASE(1, 1)
+#undef SARBP_FP64_CASE
+    return 0;
 }
 
 cudaError_t launch_bp_fp64(const BpLaunch &L, const TileConfig &tc, size_t smem, cudaStream_t s) {

@@ -126,6 +126,54 @@ __device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, uint32_t w_a
     }
 }
 
+// Store (or add, L.accumulate) a thread's MX x 2 pixels of the tile at
+// (tx0, ty0, slice zz) into the complex64 image.
+template <int MX>
+__device__ __forceinline__ void store_pixels(const BpLaunch &L, int tx0, int ty0, int zz, int warp, int lane,
+                                             const float (&re)[MX][2], const float (&im)[MX][2]) {
+    float2 *img = static_cast<float2 *>(L.img);
+#pragma unroll
+    for (int k = 0; k < MX; ++k) {
+        const int row = tx0 + warp + 8 * k;
+        const int col = ty0 + 2 * lane;
+        if (row >= L.nx || col >= L.ny) continue;
+        const long long o = (static_cast<long long>(zz) * L.nx + row) * L.ny + col;
+        if (L.vec_store && col + 1 < L.ny) {
+            float4 v = make_float4(re[k][0], im[k][0], re[k][1], im[k][1]);
+            float4 *dst = reinterpret_cast<float4 *>(img + o);
+            if (L.accumulate) {
+                const float4 old = *dst;
+                v.x += old.x;
+                v.y += old.y;
+                v.z += old.z;
+                v.w += old.w;
+            }
+            *dst = v;
+        } else {
+            float2 v0 = make_float2(re[k][0], im[k][0]);
+            if (L.accumulate) {
+                const float2 old = img[o];
+                v0.x += old.x;
+                v0.y += old.y;
+            }
+            img[o] = v0;
+            if (col + 1 < L.ny) {
+                float2 v1 = make_float2(re[k][1], im[k][1]);
+                if (L.accumulate) {
+                    const float2 old = img[o + 1];
+                    v1.x += old.x;
+                    v1.y += old.y;
+                }
+                img[o + 1] = v1;
+            }
+        }
+    }
+}
+
+// Tile-local index of pixel pair (row warp + 8k, columns 2 lane, 2 lane + 1)
+// in a partial-sum slot of TX x 64 complex64 values.
+__device__ __forceinline__ int slot_pair(int warp, int lane, int k) { return (warp + 8 * k) * kTY + 2 * lane; }
+
 template <int MX, int PB, bool CHECKED, int MINB>
 __global__ void __launch_bounds__(kThreads, MINB) bp_mixed_kernel(const BpLaunch L) {
     constexpr int TX = 8 * MX;
@@ -139,12 +187,13 @@ __global__ void __launch_bounds__(kThreads, MINB) bp_mixed_kernel(const BpLaunch
     const uint32_t pulse_bytes = static_cast<uint32_t>(wsize) * 16u;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int hyp = blockIdx.z / L.nz;  // blockIdx.z = hypothesis * nz + z-slice
-    const int ty0 = blockIdx.x * kTY, tx0 = blockIdx.y * TX, iz = blockIdx.z - hyp * L.nz;
-    const long long goff = static_cast<long long>(hyp) * L.np;
-    const double cx = L.left + static_cast<double>(tx0 + TX / 2) * L.dx;
-    const double cy = L.bottom + static_cast<double>(ty0 + kTY / 2) * L.dy;
-    const double cz = L.zlow + static_cast<double>(iz) * L.dz;
+    // this CTA's units [lo, lo + n) of the launch's (tile, stage) units
+    const TileGrid tg = tile_grid(L, TX, PB);
+    const long long G = gridDim.x;
+    const long long lo = sk_lo(blockIdx.x, tg.units, G);
+    const int n = static_cast<int>(sk_lo(blockIdx.x + 1, tg.units, G) - lo);
+    if (n <= 0) return;
+    const int S = tg.stages;
     const int i0 = warp - TX / 2;
     const int j0 = 2 * lane - kTY / 2;
     const float lam = static_cast<float>(L.lambda);
@@ -166,7 +215,7 @@ __global__ void __launch_bounds__(kThreads, MINB) bp_mixed_kernel(const BpLaunch
         }
     }
 
-    const uint32_t bar_base = smem_addr(&bars[0]);  // stage s barrier at bar_base + 8*s
+    const uint32_t bar_base = smem_addr(&bars[0]);  // buffer s barrier at bar_base + 8*s
     if (threadIdx.x == 0) {
         mbar_init(bar_base, PB);
         mbar_init(bar_base + 8, PB);
@@ -175,20 +224,35 @@ __global__ void __launch_bounds__(kThreads, MINB) bp_mixed_kernel(const BpLaunch
     }
     __syncthreads();
 
-    const int nblocks = (L.np + PB - 1) / PB;
-    if (nblocks > 0) produce_slots<PB>(L, 0, geo, win_addr, bar_base, warp, lane, cx, cy, cz, goff);
+    // records and windows of the producer cursor's unit into buffer s (lane 0
+    // of each warp works)
+    auto produce = [&](const UnitCursor &pc, int s) {
+        if (lane != 0) return;
+        const double cx = L.left + static_cast<double>(pc.tx * TX + TX / 2) * L.dx;
+        const double cy = L.bottom + static_cast<double>(pc.ty * kTY + kTY / 2) * L.dy;
+        const double cz = L.zlow + static_cast<double>(pc.iz) * L.dz;
+        produce_slots<PB>(L, pc.b, geo + s * PB, win_addr + s * PB * pulse_bytes, bar_base + 8 * s, warp, lane, cx,
+                          cy, cz, static_cast<long long>(pc.hyp) * L.np);
+    };
+
+    UnitCursor cc, pc;  // consumer at unit i, producer at unit i + 1
+    cc.init(tg, L, lo);
+    pc = cc;
+    produce(pc, 0);
     __syncthreads();
 
     int last_issued = 0;
-    bool timed_out = false;
-    for (int b = 0; b < nblocks; ++b) {
-        const int s = b & 1;
-        if (b + 1 < nblocks) {
-            produce_slots<PB>(L, b + 1, geo + (s ^ 1) * PB, win_addr + (s ^ 1) * PB * pulse_bytes,
-                              bar_base + 8 * (s ^ 1), warp, lane, cx, cy, cz, goff);
-            last_issued = b + 1;
+    int seg = 0;                 // segments flushed so far
+    int seg_first = cc.b;        // first stage of the open segment
+    for (int i = 0; i < n; ++i) {
+        const int s = i & 1;
+        if (i + 1 < n) {
+            pc.advance(tg, L);
+            produce(pc, s ^ 1);
+            last_issued = i + 1;
         }
-        const bool ok = mbar_wait_bounded(bar_base + 8 * s, (b >> 1) & 1, L.err);
+        const int b = cc.b;
+        const bool ok = mbar_wait_bounded(bar_base + 8 * s, (i >> 1) & 1, L.err);
         if (ok) {
             const int nq = min(PB, L.np - b * PB);
             // stage summary: all PB pulses active, none gated or near-field
@@ -221,70 +285,114 @@ __global__ void __launch_bounds__(kThreads, MINB) bp_mixed_kernel(const BpLaunch
             }
         }
         if (__syncthreads_or(!ok)) {
-            timed_out = true;
-            break;
+            // let the copies already issued for the other buffer land before
+            // the CTA's shared memory goes away (again bounded)
+            if (threadIdx.x == 0 && last_issued > i)
+                mbar_wait_bounded(bar_base + 8 * (last_issued & 1), (last_issued >> 1) & 1, L.err);
+            return;
         }
-    }
-    if (timed_out) {
-        // let the copies already issued for the other stage land before the
-        // CTA's shared memory goes away (again bounded)
-        if (threadIdx.x == 0 && last_issued > 0)
-            mbar_wait_bounded(bar_base + 8 * (last_issued & 1), (last_issued >> 1) & 1, L.err);
-        return;
-    }
-
-    float2 *img = static_cast<float2 *>(L.img);
+        if (i + 1 == n || b == S - 1) {
+            // the segment of this tile ends: whole tile -> image, else -> partial slot
+            if (seg_first == 0 && b == S - 1) {
+                store_pixels<MX>(L, cc.tx * TX, cc.ty * kTY, cc.hyp * L.nz + cc.iz, warp, lane, acc_re, acc_im);
+            } else {
+                float4 *slot = static_cast<float4 *>(L.sk_partial) +
+                               (2 * static_cast<long long>(blockIdx.x) + (seg > 0 ? 1 : 0)) * (TX * kTY / 2);
 #pragma unroll
-    for (int k = 0; k < MX; ++k) {
-        const int row = tx0 + warp + 8 * k;
-        const int col = ty0 + 2 * lane;
-        if (row >= L.nx || col >= L.ny) continue;
-        const long long o = ((static_cast<long long>(hyp) * L.nz + iz) * L.nx + row) * L.ny + col;
-        if (L.vec_store && col + 1 < L.ny) {
-            float4 v = make_float4(acc_re[k][0], acc_im[k][0], acc_re[k][1], acc_im[k][1]);
-            float4 *dst = reinterpret_cast<float4 *>(img + o);
-            if (L.accumulate) {
-                const float4 old = *dst;
-                v.x += old.x;
-                v.y += old.y;
-                v.z += old.z;
-                v.w += old.w;
+                for (int k = 0; k < MX; ++k)
+                    slot[slot_pair(warp, lane, k) / 2] =
+                        make_float4(acc_re[k][0], acc_im[k][0], acc_re[k][1], acc_im[k][1]);
             }
-            *dst = v;
-        } else {
-            float2 v0 = make_float2(acc_re[k][0], acc_im[k][0]);
-            if (L.accumulate) {
-                const float2 old = img[o];
-                v0.x += old.x;
-                v0.y += old.y;
-            }
-            img[o] = v0;
-            if (col + 1 < L.ny) {
-                float2 v1 = make_float2(acc_re[k][1], acc_im[k][1]);
-                if (L.accumulate) {
-                    const float2 old = img[o + 1];
-                    v1.x += old.x;
-                    v1.y += old.y;
-                }
-                img[o + 1] = v1;
-            }
+#pragma unroll
+            for (int k = 0; k < MX; ++k)
+#pragma unroll
+                for (int l = 0; l < 2; ++l) acc_re[k][l] = acc_im[k][l] = 0.0f;
+            ++seg;
+            seg_first = 0;
+        }
+        cc.advance(tg, L);
+    }
+}
+
+// Tiles whose stages were split over several CTAs: add the CTAs' partial
+// sums in CTA order (a fixed order, so results repeat bit for bit) and store
+// the tile.  One CTA per tile; tiles held whole by one CTA return at once.
+template <int MX>
+__global__ void __launch_bounds__(kThreads) bp_sk_fixup_kernel(const BpLaunch L, long long G, int PB) {
+    constexpr int TX = 8 * MX;
+    const TileGrid tg = tile_grid(L, TX, PB);
+    const long long t = blockIdx.x;
+    const long long c0 = sk_owner(t * tg.stages, tg.units, G);
+    const long long c1 = sk_owner(t * tg.stages + tg.stages - 1, tg.units, G);
+    if (c0 == c1) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float re[MX][2], im[MX][2];
+#pragma unroll
+    for (int k = 0; k < MX; ++k)
+#pragma unroll
+        for (int l = 0; l < 2; ++l) re[k][l] = im[k][l] = 0.0f;
+    const float4 *part = static_cast<const float4 *>(L.sk_partial);
+    for (long long c = c0; c <= c1; ++c) {
+        const float4 *slot = part + sk_slot(c, t, tg, G) * (TX * kTY / 2);
+#pragma unroll
+        for (int k = 0; k < MX; ++k) {
+            const float4 v = slot[slot_pair(warp, lane, k) / 2];
+            re[k][0] += v.x;
+            im[k][0] += v.y;
+            re[k][1] += v.z;
+            im[k][1] += v.w;
         }
     }
+    int tx0, ty0, zz;
+    tile_origin(tg, t, TX, tx0, ty0, zz);
+    store_pixels<MX>(L, tx0, ty0, zz, warp, lane, re, im);
+}
+
+template <int MX, int PB, bool CHECKED, int MINB>
+cudaError_t launch_kernels(const BpLaunch &L, size_t smem, cudaStream_t s) {
+    constexpr int TX = 8 * MX;
+    auto kern = bp_mixed_kernel<MX, PB, CHECKED, MINB>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const TileGrid tg = tile_grid(L, TX, PB);
+    if (tg.units < 1) return cudaSuccess;
+    // split the units over the resident CTAs unless the tiles fill whole waves
+    long long G = tg.tiles;
+    if (L.sk_partial && L.sk_resident > 0 && tg.tiles % L.sk_resident != 0) {
+        const long long g = L.sk_resident < tg.units ? L.sk_resident : tg.units;
+        if (2 * g * TX * kTY * static_cast<long long>(sizeof(float2)) <= L.sk_slot_bytes) G = g;
+    }
+    if (G > 0x7fffffffLL) return cudaErrorInvalidValue;
+    kern<<<static_cast<unsigned>(G), kThreads, smem, s>>>(L);
+    e = cudaGetLastError();
+    if (e != cudaSuccess || G == tg.tiles) return e;
+    bp_sk_fixup_kernel<MX><<<static_cast<unsigned>(tg.tiles), kThreads, 0, s>>>(L, G, PB);
+    return cudaGetLastError();
 }
 
 template <int MX, int PB>
 cudaError_t launch_mx_pb(const BpLaunch &L, bool checked, size_t smem, cudaStream_t s) {
-    constexpr int TX = 8 * MX;
-    const dim3 grid((L.ny + kTY - 1) / kTY, (L.nx + TX - 1) / TX, L.nz * L.nhyp);
     // two CTAs per SM (128 registers) by default; one CTA per SM (up to 255
     // registers) when the stage needs more shared memory than two CTAs get
     const bool one_cta = smem > 113u * 1024u;
-    auto kern = checked ? (one_cta ? bp_mixed_kernel<MX, PB, true, 1> : bp_mixed_kernel<MX, PB, true, 2>)
-                        : (one_cta ? bp_mixed_kernel<MX, PB, false, 1> : bp_mixed_kernel<MX, PB, false, 2>);
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (e != cudaSuccess) return e;
-    kern<<<grid, kThreads, smem, s>>>(L);
-    return cudaGetLastError();
+    if (checked) return one_cta ? launch_kernels<MX, PB, true, 1>(L, smem, s) : launch_kernels<MX, PB, true, 2>(L, smem, s);
+    return one_cta ? launch_kernels<MX, PB, false, 1>(L, smem, s) : launch_kernels<MX, PB, false, 2>(L, smem, s);
+}
+
+template <int MX, int PB>
+int resident_mx_pb(size_t smem) {
+    const bool one_cta = smem > 113u * 1024u;
+    auto kern = one_cta ? bp_mixed_kernel<MX, PB, false, 1> : bp_mixed_kernel<MX, PB, false, 2>;
+    int dev = 0, sms = 0, occ = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return occ * sms;
 }
 
 }  // namespace
@@ -292,6 +400,28 @@ cudaError_t launch_mx_pb(const BpLaunch &L, bool checked, size_t smem, cudaStrea
 size_t bp_mixed_smem_bytes(const TileConfig &tc, int wsize) {
     return 32 + 2 * static_cast<size_t>(tc.pb) * sizeof(PulseGeo) +
            2 * static_cast<size_t>(tc.pb) * static_cast<size_t>(wsize) * 16;
+}
+
+int bp_mixed_resident(const TileConfig &tc, size_t smem) {
+#define SARBP_MIXED_CASE(MX_, PB_) \
+    if (tc.mx == MX_ && tc.pb == PB_) return resident_mx_pb<MX_, PB_>(smem);
+    SARBP_MIXED_CASE(4, 16)
+    SARBP_MIXED_CASE(4, 8)
+    SARBP_MIXED_CASE(4, 4)
+    SARBP_MIXED_CASE(4, 2)
+    SARBP_MIXED_CASE(4, 1)
+    SARBP_MIXED_CASE(2, 16)
+    SARBP_MIXED_CASE(2, 8)
+    SARBP_MIXED_CASE(2, 4)
+    SARBP_MIXED_CASE(2, 2)
+    SARBP_MIXED_CASE(2, 1)
+    SARBP_MIXED_CASE(1, 16)
+    SARBP_MIXED_CASE(1, 8)
+    SARBP_MIXED_CASE(1, 4)
+    SARBP_MIXED_CASE(1, 2)
+    SARBP_MIXED_CASE(1, 1)
+#undef SARBP_MIXED_CASE
+    return 0;
 }
 
 cudaError_t launch_bp_mixed(const BpLaunch &L, const TileConfig &tc, bool checked, size_t smem, cudaStream_t s) {

@@ -20,6 +20,85 @@ constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23: adding it rounds to a
 constexpr uint32_t kRoundMagicBits = 0x4B400000u;
 constexpr double kTwoPi = 6.283185307179586476925286766559;
 
+// ---- work split over (tile, pulse-stage) units ---------------------------
+//
+// Tiles are numbered t = (zz * tiles_x + tx) * tiles_y + ty (zz = hypothesis
+// * nz + z-slice) and unit u = t * stages + stage.  CTA c of G takes units
+// [lo(c), lo(c+1)), lo(c) = floor(c U / G): with G = tiles every CTA gets
+// exactly one tile; with G = the resident CTA count every SM gets the same
+// number of pulse stages, whatever the tile count (no partial last wave).
+struct TileGrid {
+    int tiles_y, tiles_x;
+    long long tiles;
+    int stages;
+    long long units;
+};
+
+__host__ __device__ __forceinline__ TileGrid tile_grid(const BpLaunch &L, int TX, int PB) {
+    TileGrid g;
+    g.tiles_y = (L.ny + kTY - 1) / kTY;
+    g.tiles_x = (L.nx + TX - 1) / TX;
+    g.tiles = static_cast<long long>(g.tiles_y) * g.tiles_x * L.nz * L.nhyp;
+    g.stages = (L.np + PB - 1) / PB;
+    g.units = g.tiles * g.stages;
+    return g;
+}
+
+__host__ __device__ __forceinline__ long long sk_lo(long long c, long long units, long long G) {
+    return c * units / G;
+}
+
+// The CTA whose range holds unit u: the largest c with lo(c) <= u.
+__device__ __forceinline__ long long sk_owner(long long u, long long units, long long G) {
+    long long c = u * G / units;
+    while (c + 1 < G && sk_lo(c + 1, units, G) <= u) ++c;
+    while (c > 0 && sk_lo(c, units, G) > u) --c;
+    return c;
+}
+
+// Partial-sum slot of CTA c's segment of tile t: its first segment (the one
+// holding unit lo(c)) uses slot 2c, a later one slot 2c + 1.
+__device__ __forceinline__ long long sk_slot(long long c, long long t, const TileGrid &g, long long G) {
+    return sk_lo(c, g.units, G) >= t * g.stages ? 2 * c : 2 * c + 1;
+}
+
+// Pixel origin (row tx0, column ty0) and hypothesis-major slice zz of tile t.
+__device__ __forceinline__ void tile_origin(const TileGrid &g, long long t, int TX, int &tx0, int &ty0, int &zz) {
+    const long long r = t / g.tiles_y;
+    ty0 = static_cast<int>(t - r * g.tiles_y) * kTY;
+    const long long q = r / g.tiles_x;
+    tx0 = static_cast<int>(r - q * g.tiles_x) * TX;
+    zz = static_cast<int>(q);
+}
+
+// Position of a unit, advanced one unit at a time without divisions: stage
+// b of the tile at tile column ty, tile row tx, z-slice iz of hypothesis hyp.
+struct UnitCursor {
+    int b, ty, tx, iz, hyp;
+
+    __device__ __forceinline__ void init(const TileGrid &g, const BpLaunch &L, long long u) {
+        const long long t = u / g.stages;
+        b = static_cast<int>(u - t * g.stages);
+        const long long r = t / g.tiles_y;
+        ty = static_cast<int>(t - r * g.tiles_y);
+        const long long q = r / g.tiles_x;
+        tx = static_cast<int>(r - q * g.tiles_x);
+        hyp = static_cast<int>(q / L.nz);
+        iz = static_cast<int>(q - static_cast<long long>(hyp) * L.nz);
+    }
+    __device__ __forceinline__ void advance(const TileGrid &g, const BpLaunch &L) {
+        if (++b < g.stages) return;
+        b = 0;
+        if (++ty < g.tiles_y) return;
+        ty = 0;
+        if (++tx < g.tiles_x) return;
+        tx = 0;
+        if (++iz < L.nz) return;
+        iz = 0;
+        ++hyp;
+    }
+};
+
 __device__ __forceinline__ PulseGeo make_geo(const BpLaunch &L, int p, long long goff, double cx, double cy,
                                              double cz) {
     PulseGeo g;

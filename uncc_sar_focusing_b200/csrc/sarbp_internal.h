@@ -29,6 +29,14 @@ struct BpLaunch {
     int vec_store;          // 16-byte aligned image and even ny
     unsigned *err;
     int nhyp;               // geometry hypotheses (mixed forward kernel): arrays [nhyp][np], images [nhyp][nz][nx][ny]
+    // Work split of the forward kernels.  The (tile, pulse-stage) units of a
+    // launch, tile-major, are divided evenly over the launch's CTAs; a tile
+    // whose stages end up on several CTAs leaves per-CTA partial sums in
+    // sk_partial (two slots of one tile each per CTA) that bp_sk_fixup adds
+    // in CTA order.  sk_partial == nullptr: one CTA per tile, no partials.
+    void *sk_partial;
+    long long sk_slot_bytes;  // bytes reserved for sk_partial (launch checks the need)
+    int sk_resident;          // CTAs of the kernel resident at once on the device (0: do not split)
 };
 
 // Tile shape of the forward kernels (see bp_mixed.cu).
@@ -50,6 +58,12 @@ cudaError_t launch_adjoint_reduce(const void *partials, long long ntiles, int np
 size_t bp_adjoint_smem_bytes(const TileConfig &tc, int wsize);
 long long bp_tile_count(const BpLaunch &L, const TileConfig &tc);
 size_t bp_fp64_smem_bytes(const TileConfig &tc, int wsize);
+// CTAs of the forward kernel for this tile and shared-memory size that are
+// resident at once on the current device (0 if the query fails).  A split
+// launch with that many CTAs needs 2 * resident * (8 mx * 64) complex values
+// of sk_partial.
+int bp_mixed_resident(const TileConfig &tc, size_t smem);
+int bp_fp64_resident(const TileConfig &tc, size_t smem);
 
 // Range compression kernels (range_compress.cu)
 cudaError_t launch_rc_prep(int precision, const void *ph, const void *fac, void *fft_buf, int K, int nfft, int np,
@@ -83,6 +97,9 @@ struct sarbp_plan {
     double *d_gout;   // adjoint output staging for host outputs [4][np] (allocated on first use)
     void *d_hyp;      // host-memory staging for hypothesis batches (allocated on first use)
     size_t hyp_bytes;
+    void *d_sk;       // partial sums of tiles split over CTAs (BpLaunch::sk_partial)
+    size_t sk_bytes;
+    int sk_resident;  // resident CTAs of the plan's forward kernel
     size_t bytes;     // device bytes held
     cufftHandle fft;
     bool fft_ok;
