@@ -476,7 +476,10 @@ def gpu_arm(args):
                     "api": "sarbp_focus_submit/sarbp_focus_wait, pinned host buffers",
                     "synchronous": {"value": world * pp / e2e_sync_s, "ms_per_step": e2e_sync_s * 1e3,
                                     "api": "sarbp_focus, pinned host buffers"}},
-            "gpu_launches": 3 * args.steps,
+            # per step: rc_prep, rc_pairs, the backprojection (+ its fix-up
+            # when the tiles are split over the resident CTAs); cuFFT's
+            # kernel is the library's, not counted
+            "gpu_launches": (2 + plan.info["kernels_per_backproject"]) * args.steps,
             "kernels": {"bp_ms": bp_ms, "range_compress_ms": rc_ms,
                         "range_compress_hbm": {"bytes": rc_bytes, "achieved_gbs": rc_bytes / (rc_ms * 1e-3) / 1e9,
                                                "peak_gbs": hbm, "peak_kind": hbm_kind,

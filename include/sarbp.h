@@ -148,6 +148,25 @@ SARBP_API int sarbp_plan_destroy(sarbp_plan *plan);
 /* Device bytes the plan holds. */
 SARBP_API int sarbp_plan_workspace_bytes(const sarbp_plan *plan, size_t *bytes);
 
+/* How the plan runs its forward backprojection: tile (8 tile_mx) x 64 pixels,
+ * stage_pulses pulses per shared-memory stage, range-bin window of
+ * window_bins entries per (tile, pulse), smem_bytes of dynamic shared memory
+ * per CTA, resident_ctas CTAs resident at once on the device, tiles per
+ * image, and kernels_per_backproject (2 when a launch's (tile, stage) units
+ * are split over the resident CTAs and a fix-up kernel adds the split tiles,
+ * else 1).  No counterpart in the reference. */
+typedef struct sarbp_plan_info {
+    int tile_mx;
+    int stage_pulses;
+    int window_bins;
+    int resident_ctas;
+    long long tiles;
+    long long smem_bytes;
+    int kernels_per_backproject;
+    int reserved[5];
+} sarbp_plan_info;
+SARBP_API int sarbp_plan_get_info(const sarbp_plan *plan, sarbp_plan_info *info);
+
 /* Range compression (cuda_sar_focusing.hpp:616-620 plus the zero pad and
  * taper of matlab/bpBasic.m:82, matlab/formImage3DSAR.m:115-116):
  *   rc_p = fftshift(ifft(w .* ph_p, nfft)) for every pulse,

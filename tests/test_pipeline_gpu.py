@@ -113,3 +113,15 @@ def test_submit_errors(F):
         out = plan.new_image()
         plan.focus_wait(plan.focus_submit(*args(a), out=out))
         np.testing.assert_array_equal(out, plan.focus(*args(a)))
+
+
+def test_plan_info_reports_the_split(F):
+    import torch  # noqa: F401
+
+    sc = scene(21)
+    with F.Plan.for_scene(sc, "mixed") as plan:
+        info = plan.info
+        assert info["tile_mx"] in (1, 2, 4) and info["stage_pulses"] >= 1
+        assert info["resident_ctas"] > 0 and info["window_bins"] >= 4
+        split = info["tiles"] % info["resident_ctas"] != 0
+        assert info["kernels_per_backproject"] == (2 if split else 1)

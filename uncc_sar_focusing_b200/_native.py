@@ -38,7 +38,7 @@ EXPORTED = (
     "sarbp_abi_version", "sarbp_status_string", "sarbp_plan_create", "sarbp_plan_destroy",
     "sarbp_plan_workspace_bytes", "sarbp_range_compress", "sarbp_get_range_profiles", "sarbp_backproject",
     "sarbp_focus", "sarbp_focus_image", "sarbp_plan_check", "sarbp_backproject_noalloc",
-    "sarbp_backproject_adjoint", "sarbp_backproject_hypotheses", "sarbp_focus_submit", "sarbp_focus_wait",
+    "sarbp_backproject_adjoint", "sarbp_backproject_hypotheses", "sarbp_focus_submit", "sarbp_focus_wait", "sarbp_plan_get_info",
 )
 
 
@@ -52,6 +52,12 @@ class PlanDesc(ctypes.Structure):
     _fields_ = [("num_range_samples", ctypes.c_int), ("num_pulses", ctypes.c_int), ("nfft", ctypes.c_int),
                 ("max_wr", ctypes.c_double), ("grid", Grid), ("precision", ctypes.c_int),
                 ("window", ctypes.c_int), ("device", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [("tile_mx", ctypes.c_int), ("stage_pulses", ctypes.c_int), ("window_bins", ctypes.c_int),
+                ("resident_ctas", ctypes.c_int), ("tiles", ctypes.c_longlong), ("smem_bytes", ctypes.c_longlong),
+                ("kernels_per_backproject", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
 
 
 class Geometry(ctypes.Structure):
@@ -92,6 +98,7 @@ def lib():
         L.sarbp_backproject_hypotheses.argtypes = [vp, P(Geometry), i, vp, i, i, vp]
         L.sarbp_focus_submit.argtypes = [vp, P(Aperture), vp, P(ctypes.c_ulonglong)]
         L.sarbp_focus_wait.argtypes = [vp, ctypes.c_ulonglong]
+        L.sarbp_plan_get_info.argtypes = [vp, P(PlanInfo)]
         for name in EXPORTED:
             if name != "sarbp_status_string":
                 getattr(L, name).restype = i

@@ -755,6 +755,21 @@ int sarbp_plan_workspace_bytes(const sarbp_plan *plan, size_t *bytes) {
     return SARBP_OK;
 }
 
+int sarbp_plan_get_info(const sarbp_plan *plan, sarbp_plan_info *info) {
+    if (!plan || !info) return SARBP_ERR_NULL_POINTER;
+    std::memset(info, 0, sizeof(*info));
+    const sarbp_grid &g = plan->desc.grid;
+    info->tile_mx = plan->tile.mx;
+    info->stage_pulses = plan->tile.pb;
+    info->window_bins = plan->wsize;
+    info->resident_ctas = plan->sk_resident;
+    info->tiles = static_cast<long long>((g.ny + 63) / 64) * ((g.nx + 8 * plan->tile.mx - 1) / (8 * plan->tile.mx)) *
+                  g.nz;
+    info->smem_bytes = static_cast<long long>(plan->smem);
+    info->kernels_per_backproject = (plan->d_sk && plan->sk_resident > 0 && info->tiles % plan->sk_resident != 0) ? 2 : 1;
+    return SARBP_OK;
+}
+
 int sarbp_range_compress(sarbp_plan *plan, const void *phase_history, int num_pulses, int memory, void *stream) {
     if (!plan) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);

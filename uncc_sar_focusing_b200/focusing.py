@@ -107,6 +107,13 @@ class Plan:
         N.check(N.lib().sarbp_plan_workspace_bytes(self._h, ctypes.byref(v)), "sarbp_plan_workspace_bytes")
         return int(v.value)
 
+    @property
+    def info(self) -> dict:
+        """Tiling the plan chose (sarbp_plan_get_info)."""
+        v = N.PlanInfo()
+        N.check(N.lib().sarbp_plan_get_info(self._h, ctypes.byref(v)), "sarbp_plan_get_info")
+        return {f: getattr(v, f) for f, _ in N.PlanInfo._fields_ if f != "reserved"}
+
     def image_shape(self):
         g = self.grid
         return (g.nz, g.nx, g.ny)
