@@ -233,6 +233,45 @@ SARBP_API int sarbp_focus_submit(sarbp_plan *plan, const sarbp_aperture *apertur
                                  unsigned long long *ticket);
 SARBP_API int sarbp_focus_wait(sarbp_plan *plan, unsigned long long ticket);
 
+/* Batches of independent scenes of uneven sizes (different K, pulse counts,
+ * nfft, grids) focused together: one range-compression launch pair for all
+ * scenes (plus one FFT per scene) and ONE backprojection launch whose
+ * (tile, pulse-stage) units of all scenes are split evenly over the resident
+ * CTAs, captured once as a CUDA graph and replayed per call.  The reference
+ * focuses one aperture per call (cuda_sar_focusing.hpp:526-723).
+ * descs[i] describes scene i (precision must be SARBP_PRECISION_MIXED; all
+ * on descs[0].device).  sarbp_batch_focus takes DEVICE phase histories,
+ * geometry and images (complex64 on scene i's grid), num_pulses <= the
+ * scene's num_pulses; it is stream-ordered and waits only for the batch's
+ * previous call before reusing its scene table.  sarbp_batch_wait waits for
+ * the last call, returns kernel-side errors, and (if image_ms is not NULL)
+ * stores each image's completion time in ms after the call's start, from the
+ * GPU clock.  sarbp_batch_autotune times every instantiated tile shape on
+ * the given inputs (each run focuses them), keeps the fastest and returns
+ * its time per batch. */
+typedef struct sarbp_batch sarbp_batch;
+typedef struct sarbp_batch_info {
+    int num_scenes;
+    int tile_mx;
+    int stage_pulses;
+    int max_window_bins;
+    int resident_ctas;
+    int graph;              /* 1: calls replay a captured CUDA graph */
+    long long tiles;        /* of the last call */
+    long long units;        /* (tile, stage) units of the last call */
+    long long smem_bytes;
+    long long workspace_bytes;
+    int reserved[4];
+} sarbp_batch_info;
+SARBP_API int sarbp_batch_create(const sarbp_plan_desc *descs, int num_scenes, sarbp_batch **batch);
+SARBP_API int sarbp_batch_destroy(sarbp_batch *batch);
+SARBP_API int sarbp_batch_focus(sarbp_batch *batch, const sarbp_aperture *apertures, void *const *images,
+                                void *stream);
+SARBP_API int sarbp_batch_wait(sarbp_batch *batch, double *image_ms);
+SARBP_API int sarbp_batch_autotune(sarbp_batch *batch, const sarbp_aperture *apertures, void *const *images,
+                                   void *stream, double *best_ms);
+SARBP_API int sarbp_batch_get_info(const sarbp_batch *batch, sarbp_batch_info *info);
+
 /* One call, no plan kept: create, focus, destroy (host or device buffers). */
 SARBP_API int sarbp_focus_image(const sarbp_plan_desc *desc, const sarbp_aperture *aperture, void *image,
                       int image_memory);

@@ -39,6 +39,8 @@ EXPORTED = (
     "sarbp_plan_workspace_bytes", "sarbp_range_compress", "sarbp_get_range_profiles", "sarbp_backproject",
     "sarbp_focus", "sarbp_focus_image", "sarbp_plan_check", "sarbp_backproject_noalloc",
     "sarbp_backproject_adjoint", "sarbp_backproject_hypotheses", "sarbp_focus_submit", "sarbp_focus_wait", "sarbp_plan_get_info",
+    "sarbp_batch_create", "sarbp_batch_destroy", "sarbp_batch_focus", "sarbp_batch_wait", "sarbp_batch_autotune",
+    "sarbp_batch_get_info",
 )
 
 
@@ -58,6 +60,13 @@ class PlanInfo(ctypes.Structure):
     _fields_ = [("tile_mx", ctypes.c_int), ("stage_pulses", ctypes.c_int), ("window_bins", ctypes.c_int),
                 ("resident_ctas", ctypes.c_int), ("tiles", ctypes.c_longlong), ("smem_bytes", ctypes.c_longlong),
                 ("kernels_per_backproject", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("num_scenes", ctypes.c_int), ("tile_mx", ctypes.c_int), ("stage_pulses", ctypes.c_int),
+                ("max_window_bins", ctypes.c_int), ("resident_ctas", ctypes.c_int), ("graph", ctypes.c_int),
+                ("tiles", ctypes.c_longlong), ("units", ctypes.c_longlong), ("smem_bytes", ctypes.c_longlong),
+                ("workspace_bytes", ctypes.c_longlong), ("reserved", ctypes.c_int * 4)]
 
 
 class Geometry(ctypes.Structure):
@@ -99,6 +108,12 @@ def lib():
         L.sarbp_focus_submit.argtypes = [vp, P(Aperture), vp, P(ctypes.c_ulonglong)]
         L.sarbp_focus_wait.argtypes = [vp, ctypes.c_ulonglong]
         L.sarbp_plan_get_info.argtypes = [vp, P(PlanInfo)]
+        L.sarbp_batch_create.argtypes = [P(PlanDesc), i, P(vp)]
+        L.sarbp_batch_destroy.argtypes = [vp]
+        L.sarbp_batch_focus.argtypes = [vp, P(Aperture), P(vp), vp]
+        L.sarbp_batch_wait.argtypes = [vp, P(ctypes.c_double)]
+        L.sarbp_batch_autotune.argtypes = [vp, P(Aperture), P(vp), vp, P(ctypes.c_double)]
+        L.sarbp_batch_get_info.argtypes = [vp, P(BatchInfo)]
         for name in EXPORTED:
             if name != "sarbp_status_string":
                 getattr(L, name).restype = i

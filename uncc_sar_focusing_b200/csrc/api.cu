@@ -14,96 +14,18 @@
 #include <vector>
 
 #include "bp_common.cuh"
+#include "host_common.h"
 #include "sarbp_internal.h"
 
 using namespace sarbp;
+using namespace sarbp::host;
 
 namespace {
 
-int from_cuda(cudaError_t e) {
-    if (e == cudaSuccess) return SARBP_OK;
-    if (e == cudaErrorMemoryAllocation) return SARBP_ERR_OUT_OF_MEMORY;
-    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return SARBP_ERR_NO_DEVICE;
-    return SARBP_ERR_CUDA;
-}
-
-int from_cufft(cufftResult r) {
-    if (r == CUFFT_SUCCESS) return SARBP_OK;
-    if (r == CUFFT_ALLOC_FAILED) return SARBP_ERR_OUT_OF_MEMORY;
-    return SARBP_ERR_CUFFT;
-}
-
-#define SARBP_TRY(call)                       \
-    do {                                      \
-        const int st_ = (call);               \
-        if (st_ != SARBP_OK) return st_;      \
-    } while (0)
-
-#define SARBP_TRY_CUDA(call)                  \
-    do {                                      \
-        const cudaError_t e_ = (call);        \
-        if (e_ != cudaSuccess) {              \
-            cudaGetLastError();               \
-            return from_cuda(e_);             \
-        }                                     \
-    } while (0)
-
-// Makes plan->device current for the duration of a call and restores the
-// caller's device afterwards.
-struct DeviceGuard {
-    int prev = -1;
-    bool changed = false;
-    cudaError_t status = cudaSuccess;
-    explicit DeviceGuard(int dev) {
-        status = cudaGetDevice(&prev);
-        if (status == cudaSuccess && prev != dev) {
-            status = cudaSetDevice(dev);
-            changed = status == cudaSuccess;
-        }
-    }
-    ~DeviceGuard() {
-        if (changed) cudaSetDevice(prev);
-    }
-};
-
-bool finite_nonneg(double v) { return std::isfinite(v) && v >= 0.0; }
-
-int validate_desc(const sarbp_plan_desc *d) {
-    if (!d) return SARBP_ERR_NULL_POINTER;
-    const sarbp_grid &g = d->grid;
-    if (d->num_range_samples < 1 || d->num_pulses < 1 || d->nfft < 2 || d->nfft < d->num_range_samples ||
-        d->nfft > (1 << 24))
-        return SARBP_ERR_INVALID_ARGUMENT;
-    if (!(std::isfinite(d->max_wr) && d->max_wr > 0.0)) return SARBP_ERR_INVALID_ARGUMENT;
-    if (g.nx < 1 || g.ny < 1 || g.nz < 1 || g.nx > (1 << 20) || g.ny > (1 << 20) || g.nz > 65535)
-        return SARBP_ERR_INVALID_ARGUMENT;
-    if (!(std::isfinite(g.x0) && std::isfinite(g.y0) && std::isfinite(g.z0) && finite_nonneg(g.wx) &&
-          finite_nonneg(g.wy) && finite_nonneg(g.wz)))
-        return SARBP_ERR_INVALID_ARGUMENT;
-    if (d->precision != SARBP_PRECISION_MIXED && d->precision != SARBP_PRECISION_FP64)
-        return SARBP_ERR_INVALID_ARGUMENT;
-    if (d->window != SARBP_WINDOW_NONE && d->window != SARBP_WINDOW_HAMMING) return SARBP_ERR_INVALID_ARGUMENT;
-    const double samples = static_cast<double>(d->num_pulses) * static_cast<double>(d->nfft);
-    if (samples > 4.0e9) return SARBP_ERR_UNSUPPORTED;
-    return SARBP_OK;
-}
-
-void axis(int n, double c, double w, double *lo, double *step) {
-    if (n > 1) {
-        *step = w / static_cast<double>(n - 1);
-        *lo = c - 0.5 * w;
-    } else {
-        *step = 0.0;
-        *lo = c;
-    }
-}
-
 // Window geometry for a tile of (8*mx) x 64 pixels centred on an integer pixel.
 void window_for(const sarbp_plan *p, int mx, int *W, int *wsize) {
-    const double hx = 0.5 * 8.0 * mx * p->dx, hy = 0.5 * 64.0 * p->dy;
-    const double hd = std::sqrt(hx * hx + hy * hy);
-    *W = static_cast<int>(std::ceil(p->lambda * hd)) + 3;
-    *wsize = 2 * (*W) + 2;
+    double hd;
+    tile_window(p->lambda, p->dx, p->dy, mx, W, wsize, &hd);
 }
 
 // Largest stage depth whose shared memory fits 2 CTAs per SM (mixed) or one
@@ -221,13 +143,6 @@ int check_geometry_host(const sarbp_geometry *g) {
     for (const double *a : arrs)
         for (int i = 0; i < g->num_pulses; ++i)
             if (!std::isfinite(a[i])) return SARBP_ERR_NOT_FINITE;
-    return SARBP_OK;
-}
-
-int status_from_bits(unsigned bits) {
-    if (bits & ERRBIT_TIMEOUT) return SARBP_ERR_KERNEL_TIMEOUT;
-    if (bits & ERRBIT_NOT_FINITE) return SARBP_ERR_NOT_FINITE;
-    if (bits & ERRBIT_BOUNDS) return SARBP_ERR_KERNEL_BOUNDS;
     return SARBP_OK;
 }
 
@@ -661,12 +576,10 @@ int sarbp_plan_create(const sarbp_plan_desc *desc, sarbp_plan **out) {
         return st;
     }
     {
-        const double hx = 0.5 * 8.0 * p->tile.mx * p->dx, hy = 0.5 * 64.0 * p->dy;
-        const double hd = std::sqrt(hx * hx + hy * hy);
-        // far-field remainder error <= 0.625 hd^4 / Rc^3 metres; keep k times
-        // it under 1e-7 revolutions, else the pulse takes the exact path
-        p->near_hd16 = 16.0 * hd;
-        p->near_coef = 0.625 * hd * hd * hd * hd / 1.0e-7;
+        int W, wsize;
+        double hd;
+        tile_window(p->lambda, p->dx, p->dy, p->tile.mx, &W, &wsize, &hd);
+        near_field_consts(hd, &p->near_hd16, &p->near_coef);
     }
     p->guard = p->wsize + 2;
     p->row_stride = static_cast<long long>(p->nfft) + 2LL * p->guard;
@@ -704,18 +617,7 @@ int sarbp_plan_create(const sarbp_plan_desc *desc, sarbp_plan **out) {
     }
     // fac[k] = w_k / nfft * exp(+j 2 pi ((k s) mod nfft) / nfft), s = (nfft+1)/2
     {
-        const int K = p->K, N = p->nfft;
-        const long long s = (N + 1) / 2;
-        std::vector<double> fac(2 * static_cast<size_t>(K));
-        for (int k = 0; k < K; ++k) {
-            double w = 1.0;
-            if (desc->window == SARBP_WINDOW_HAMMING && K > 1)
-                w = 0.54 - 0.46 * std::cos(2.0 * M_PI * static_cast<double>(k) / static_cast<double>(K - 1));
-            const long long m = (static_cast<long long>(k) * s) % N;
-            const double ang = 2.0 * M_PI * static_cast<double>(m) / static_cast<double>(N);
-            fac[2 * k] = w / N * std::cos(ang);
-            fac[2 * k + 1] = w / N * std::sin(ang);
-        }
+        const std::vector<double> fac = range_factors(*desc);
         cudaError_t e;
         if (p->precision == SARBP_PRECISION_FP64) {
             e = cudaMemcpy(p->d_fac, fac.data(), fac.size() * sizeof(double), cudaMemcpyHostToDevice);

@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(kThreads) bp_sk_fixup64_kernel(const BpLaunch 
         for (int l = 0; l < 2; ++l) re[k][l] = im[k][l] = 0.0;
     const double2 *part = static_cast<const double2 *>(L.sk_partial);
     for (long long c = c0; c <= c1; ++c) {
-        const double2 *slot = part + tile::sk_slot(c, t, tg, G) * (TX * kTY);
+        const double2 *slot = part + tile::sk_slot(c, t * tg.stages, tg.units, G) * (TX * kTY);
 #pragma unroll
         for (int k = 0; k < MX; ++k)
 #pragma unroll

@@ -174,8 +174,56 @@ __device__ __forceinline__ void store_pixels(const BpLaunch &L, int tx0, int ty0
 // in a partial-sum slot of TX x 64 complex64 values.
 __device__ __forceinline__ int slot_pair(int warp, int lane, int k) { return (warp + 8 * k) * kTY + 2 * lane; }
 
-template <int MX, int PB, bool CHECKED, int MINB>
-__global__ void __launch_bounds__(kThreads, MINB) bp_mixed_kernel(const BpLaunch L) {
+// Unit cursor over one launch (BATCH = false: the kernel parameter's scene)
+// or over the scenes of a batch table, scene-major.
+template <int TX, int PB, bool BATCH>
+struct SceneCursor {
+    const BpLaunch *L;
+    TileGrid g;
+    UnitCursor u;
+    int scene;
+
+    __device__ __forceinline__ void init(const BpLaunch *L0, const BatchScene *scenes, int nscenes, long long unit) {
+        scene = 0;
+        L = L0;
+        if constexpr (BATCH) {
+            int a = 0, z = nscenes - 1;  // last scene with unit_begin <= unit
+            while (a < z) {
+                const int m = (a + z + 1) >> 1;
+                if (scenes[m].unit_begin <= unit) a = m;
+                else z = m - 1;
+            }
+            scene = a;
+            L = &scenes[a].L;
+            unit -= scenes[a].unit_begin;
+        }
+        g = tile_grid(*L, TX, PB);
+        u.init(g, *L, unit);
+    }
+    // true when the cursor moved on to the next scene
+    __device__ __forceinline__ bool advance(const BatchScene *scenes, int nscenes) {
+        u.advance(g, *L);
+        if constexpr (BATCH) {
+            if (u.hyp >= L->nhyp && scene + 1 < nscenes) {
+                ++scene;
+                L = &scenes[scene].L;
+                g = tile_grid(*L, TX, PB);
+                u.b = u.ty = u.tx = u.iz = u.hyp = 0;
+                return true;
+            }
+        }
+        return false;
+    }
+};
+
+// BATCH = false: one scene, L0.  BATCH = true: the scenes of the table; L0
+// carries only the batch-wide window size (the largest scene window: the
+// stage buffers' stride) and sk_partial; each scene's image completion time
+// goes to done[scene].
+template <int MX, int PB, bool CHECKED, int MINB, bool BATCH>
+__global__ void __launch_bounds__(kThreads, MINB)
+    bp_mixed_kernel(const __grid_constant__ BpLaunch L0, const BatchScene *__restrict__ scenes, int nscenes,
+                    long long batch_units, unsigned long long *__restrict__ done) {
     constexpr int TX = 8 * MX;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
@@ -183,37 +231,46 @@ __global__ void __launch_bounds__(kThreads, MINB) bp_mixed_kernel(const BpLaunch
     PulseGeo *geo = reinterpret_cast<PulseGeo *>(smem + 32);
     const uint32_t win_addr = smem_addr(smem + 32 + 2 * PB * sizeof(PulseGeo));
     const uint32_t zero_addr = smem_addr(zero);
-    const int wsize = L.wsize;
-    const uint32_t pulse_bytes = static_cast<uint32_t>(wsize) * 16u;
+    const uint32_t buf_bytes = static_cast<uint32_t>(PB) * static_cast<uint32_t>(L0.wsize) * 16u;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // this CTA's units [lo, lo + n) of the launch's (tile, stage) units
-    const TileGrid tg = tile_grid(L, TX, PB);
+    const long long U = BATCH ? batch_units : tile_grid(L0, TX, PB).units;
     const long long G = gridDim.x;
-    const long long lo = sk_lo(blockIdx.x, tg.units, G);
-    const int n = static_cast<int>(sk_lo(blockIdx.x + 1, tg.units, G) - lo);
+    const long long lo = sk_lo(blockIdx.x, U, G);
+    const int n = static_cast<int>(sk_lo(blockIdx.x + 1, U, G) - lo);
     if (n <= 0) return;
-    const int S = tg.stages;
     const int i0 = warp - TX / 2;
     const int j0 = 2 * lane - kTY / 2;
-    const float lam = static_cast<float>(L.lambda);
 
+    SceneCursor<TX, PB, BATCH> cc, pc;  // consumer at unit i, producer at unit i + 1
+    cc.init(&L0, scenes, nscenes, lo);
+    pc = cc;
+
+    // per-scene constants of the consumer
     float2 nd2[MX];  // -|d|^2 of the thread's pixel pairs
-    float acc_re[MX][2], acc_im[MX][2];
-    {
+    float lam;
+    int wsize;
+    uint32_t pulse_bytes;
+    auto scene_consts = [&]() {
+        const BpLaunch &L = *cc.L;
+        lam = static_cast<float>(L.lambda);
+        wsize = L.wsize;
+        pulse_bytes = static_cast<uint32_t>(wsize) * 16u;
         const float dxf = static_cast<float>(L.dx), dyf = static_cast<float>(L.dy);
 #pragma unroll
         for (int k = 0; k < MX; ++k) {
             const float di = static_cast<float>(i0 + 8 * k) * dxf;
             const float dj0 = static_cast<float>(j0) * dyf, dj1 = static_cast<float>(j0 + 1) * dyf;
             nd2[k] = make_float2(-fmaf(di, di, dj0 * dj0), -fmaf(di, di, dj1 * dj1));
-#pragma unroll
-            for (int l = 0; l < 2; ++l) {
-                acc_re[k][l] = 0.0f;
-                acc_im[k][l] = 0.0f;
-            }
         }
-    }
+    };
+    scene_consts();
+    float acc_re[MX][2], acc_im[MX][2];
+#pragma unroll
+    for (int k = 0; k < MX; ++k)
+#pragma unroll
+        for (int l = 0; l < 2; ++l) acc_re[k][l] = acc_im[k][l] = 0.0f;
 
     const uint32_t bar_base = smem_addr(&bars[0]);  // buffer s barrier at bar_base + 8*s
     if (threadIdx.x == 0) {
@@ -226,32 +283,32 @@ __global__ void __launch_bounds__(kThreads, MINB) bp_mixed_kernel(const BpLaunch
 
     // records and windows of the producer cursor's unit into buffer s (lane 0
     // of each warp works)
-    auto produce = [&](const UnitCursor &pc, int s) {
+    auto produce = [&](int s) {
         if (lane != 0) return;
-        const double cx = L.left + static_cast<double>(pc.tx * TX + TX / 2) * L.dx;
-        const double cy = L.bottom + static_cast<double>(pc.ty * kTY + kTY / 2) * L.dy;
-        const double cz = L.zlow + static_cast<double>(pc.iz) * L.dz;
-        produce_slots<PB>(L, pc.b, geo + s * PB, win_addr + s * PB * pulse_bytes, bar_base + 8 * s, warp, lane, cx,
-                          cy, cz, static_cast<long long>(pc.hyp) * L.np);
+        const BpLaunch &L = *pc.L;
+        const double cx = L.left + static_cast<double>(pc.u.tx * TX + TX / 2) * L.dx;
+        const double cy = L.bottom + static_cast<double>(pc.u.ty * kTY + kTY / 2) * L.dy;
+        const double cz = L.zlow + static_cast<double>(pc.u.iz) * L.dz;
+        produce_slots<PB>(L, pc.u.b, geo + s * PB, win_addr + s * buf_bytes, bar_base + 8 * s, warp, lane, cx, cy,
+                          cz, static_cast<long long>(pc.u.hyp) * L.np);
     };
 
-    UnitCursor cc, pc;  // consumer at unit i, producer at unit i + 1
-    cc.init(tg, L, lo);
-    pc = cc;
-    produce(pc, 0);
+    produce(0);
     __syncthreads();
 
     int last_issued = 0;
     int seg = 0;                 // segments flushed so far
-    int seg_first = cc.b;        // first stage of the open segment
+    int seg_first = cc.u.b;      // first stage of the open segment
     for (int i = 0; i < n; ++i) {
         const int s = i & 1;
         if (i + 1 < n) {
-            pc.advance(tg, L);
-            produce(pc, s ^ 1);
+            pc.advance(scenes, nscenes);
+            produce(s ^ 1);
             last_issued = i + 1;
         }
-        const int b = cc.b;
+        const BpLaunch &L = *cc.L;
+        const int S = cc.g.stages;
+        const int b = cc.u.b;
         const bool ok = mbar_wait_bounded(bar_base + 8 * s, (i >> 1) & 1, L.err);
         if (ok) {
             const int nq = min(PB, L.np - b * PB);
@@ -259,7 +316,7 @@ __global__ void __launch_bounds__(kThreads, MINB) bp_mixed_kernel(const BpLaunch
             const int my_flags = lane < nq ? geo[s * PB + lane].flags : 0;
             const int any_f = __reduce_or_sync(0xffffffffu, my_flags);
             const int all_f = __reduce_and_sync(0xffffffffu, lane < nq ? my_flags : PG_ACTIVE);
-            const uint32_t w0 = win_addr + s * PB * pulse_bytes;
+            const uint32_t w0 = win_addr + s * buf_bytes;
             if (nq == PB && (all_f & PG_ACTIVE) && !(any_f & (PG_GATE | PG_NEAR))) {
                 constexpr int kUnroll = kFastUnroll > 0 ? kFastUnroll : PB;
 #pragma unroll kUnroll
@@ -294,9 +351,14 @@ __global__ void __launch_bounds__(kThreads, MINB) bp_mixed_kernel(const BpLaunch
         if (i + 1 == n || b == S - 1) {
             // the segment of this tile ends: whole tile -> image, else -> partial slot
             if (seg_first == 0 && b == S - 1) {
-                store_pixels<MX>(L, cc.tx * TX, cc.ty * kTY, cc.hyp * L.nz + cc.iz, warp, lane, acc_re, acc_im);
+                store_pixels<MX>(L, cc.u.tx * TX, cc.u.ty * kTY, cc.u.hyp * L.nz + cc.u.iz, warp, lane, acc_re,
+                                 acc_im);
+                if (BATCH && done) {
+                    __syncthreads();
+                    if (threadIdx.x == 0) atomicMax(done + cc.scene, global_timer_ns());
+                }
             } else {
-                float4 *slot = static_cast<float4 *>(L.sk_partial) +
+                float4 *slot = static_cast<float4 *>(L0.sk_partial) +
                                (2 * static_cast<long long>(blockIdx.x) + (seg > 0 ? 1 : 0)) * (TX * kTY / 2);
 #pragma unroll
                 for (int k = 0; k < MX; ++k)
@@ -310,20 +372,39 @@ __global__ void __launch_bounds__(kThreads, MINB) bp_mixed_kernel(const BpLaunch
             ++seg;
             seg_first = 0;
         }
-        cc.advance(tg, L);
+        if (cc.advance(scenes, nscenes)) scene_consts();
     }
 }
 
 // Tiles whose stages were split over several CTAs: add the CTAs' partial
 // sums in CTA order (a fixed order, so results repeat bit for bit) and store
-// the tile.  One CTA per tile; tiles held whole by one CTA return at once.
-template <int MX>
-__global__ void __launch_bounds__(kThreads) bp_sk_fixup_kernel(const BpLaunch L, long long G, int PB) {
+// the tile.  One CTA per tile of the launch; tiles held whole by one CTA
+// return at once.
+template <int MX, int PB, bool BATCH>
+__global__ void __launch_bounds__(kThreads)
+    bp_sk_fixup_kernel(const __grid_constant__ BpLaunch L0, const BatchScene *__restrict__ scenes, int nscenes,
+                       long long units, long long G, unsigned long long *__restrict__ done) {
     constexpr int TX = 8 * MX;
+    long long t = blockIdx.x, unit0 = 0;
+    const BpLaunch *Lp = &L0;
+    int scene = 0;
+    if constexpr (BATCH) {
+        int a = 0, z = nscenes - 1;  // last scene with tile_begin <= t
+        while (a < z) {
+            const int m = (a + z + 1) >> 1;
+            if (scenes[m].tile_begin <= t) a = m;
+            else z = m - 1;
+        }
+        scene = a;
+        Lp = &scenes[a].L;
+        t -= scenes[a].tile_begin;
+        unit0 = scenes[a].unit_begin;
+    }
+    const BpLaunch &L = *Lp;
     const TileGrid tg = tile_grid(L, TX, PB);
-    const long long t = blockIdx.x;
-    const long long c0 = sk_owner(t * tg.stages, tg.units, G);
-    const long long c1 = sk_owner(t * tg.stages + tg.stages - 1, tg.units, G);
+    const long long first = unit0 + t * tg.stages;
+    const long long c0 = sk_owner(first, units, G);
+    const long long c1 = sk_owner(first + tg.stages - 1, units, G);
     if (c0 == c1) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float re[MX][2], im[MX][2];
@@ -331,9 +412,9 @@ __global__ void __launch_bounds__(kThreads) bp_sk_fixup_kernel(const BpLaunch L,
     for (int k = 0; k < MX; ++k)
 #pragma unroll
         for (int l = 0; l < 2; ++l) re[k][l] = im[k][l] = 0.0f;
-    const float4 *part = static_cast<const float4 *>(L.sk_partial);
+    const float4 *part = static_cast<const float4 *>(L0.sk_partial);
     for (long long c = c0; c <= c1; ++c) {
-        const float4 *slot = part + sk_slot(c, t, tg, G) * (TX * kTY / 2);
+        const float4 *slot = part + sk_slot(c, first, units, G) * (TX * kTY / 2);
 #pragma unroll
         for (int k = 0; k < MX; ++k) {
             const float4 v = slot[slot_pair(warp, lane, k) / 2];
@@ -346,12 +427,16 @@ __global__ void __launch_bounds__(kThreads) bp_sk_fixup_kernel(const BpLaunch L,
     int tx0, ty0, zz;
     tile_origin(tg, t, TX, tx0, ty0, zz);
     store_pixels<MX>(L, tx0, ty0, zz, warp, lane, re, im);
+    if (BATCH && done) {
+        __syncthreads();
+        if (threadIdx.x == 0) atomicMax(done + scene, global_timer_ns());
+    }
 }
 
 template <int MX, int PB, bool CHECKED, int MINB>
 cudaError_t launch_kernels(const BpLaunch &L, size_t smem, cudaStream_t s) {
     constexpr int TX = 8 * MX;
-    auto kern = bp_mixed_kernel<MX, PB, CHECKED, MINB>;
+    auto kern = bp_mixed_kernel<MX, PB, CHECKED, MINB, false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     const TileGrid tg = tile_grid(L, TX, PB);
@@ -363,10 +448,11 @@ cudaError_t launch_kernels(const BpLaunch &L, size_t smem, cudaStream_t s) {
         if (2 * g * TX * kTY * static_cast<long long>(sizeof(float2)) <= L.sk_slot_bytes) G = g;
     }
     if (G > 0x7fffffffLL) return cudaErrorInvalidValue;
-    kern<<<static_cast<unsigned>(G), kThreads, smem, s>>>(L);
+    kern<<<static_cast<unsigned>(G), kThreads, smem, s>>>(L, nullptr, 0, 0, nullptr);
     e = cudaGetLastError();
     if (e != cudaSuccess || G == tg.tiles) return e;
-    bp_sk_fixup_kernel<MX><<<static_cast<unsigned>(tg.tiles), kThreads, 0, s>>>(L, G, PB);
+    bp_sk_fixup_kernel<MX, PB, false>
+        <<<static_cast<unsigned>(tg.tiles), kThreads, 0, s>>>(L, nullptr, 0, tg.units, G, nullptr);
     return cudaGetLastError();
 }
 
@@ -379,10 +465,8 @@ cudaError_t launch_mx_pb(const BpLaunch &L, bool checked, size_t smem, cudaStrea
     return one_cta ? launch_kernels<MX, PB, false, 1>(L, smem, s) : launch_kernels<MX, PB, false, 2>(L, smem, s);
 }
 
-template <int MX, int PB>
-int resident_mx_pb(size_t smem) {
-    const bool one_cta = smem > 113u * 1024u;
-    auto kern = one_cta ? bp_mixed_kernel<MX, PB, false, 1> : bp_mixed_kernel<MX, PB, false, 2>;
+template <typename K>
+int resident_of(K kern, size_t smem) {
     int dev = 0, sms = 0, occ = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
@@ -393,6 +477,44 @@ int resident_mx_pb(size_t smem) {
         return 0;
     }
     return occ * sms;
+}
+
+template <int MX, int PB>
+int resident_mx_pb(size_t smem) {
+    const bool one_cta = smem > 113u * 1024u;
+    return one_cta ? resident_of(bp_mixed_kernel<MX, PB, false, 1, false>, smem)
+                   : resident_of(bp_mixed_kernel<MX, PB, false, 2, false>, smem);
+}
+
+template <int MX, int PB, int MINB>
+cudaError_t launch_batch_kernels(const BatchScene *scenes, int nscenes, long long units, long long tiles,
+                                 size_t smem, int resident, const BpLaunch &L0, unsigned long long *done,
+                                 cudaStream_t s) {
+    auto kern = bp_mixed_kernel<MX, PB, false, MINB, true>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const long long G = resident < units ? resident : units;
+    if (G < 1 || G > 0x7fffffffLL || tiles > 0x7fffffffLL) return cudaErrorInvalidValue;
+    kern<<<static_cast<unsigned>(G), kThreads, smem, s>>>(L0, scenes, nscenes, units, done);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    bp_sk_fixup_kernel<MX, PB, true>
+        <<<static_cast<unsigned>(tiles), kThreads, 0, s>>>(L0, scenes, nscenes, units, G, done);
+    return cudaGetLastError();
+}
+
+template <int MX, int PB>
+cudaError_t launch_batch_mx_pb(const BatchScene *scenes, int nscenes, long long units, long long tiles, size_t smem,
+                               int resident, const BpLaunch &L0, unsigned long long *done, cudaStream_t s) {
+    return smem > 113u * 1024u
+               ? launch_batch_kernels<MX, PB, 1>(scenes, nscenes, units, tiles, smem, resident, L0, done, s)
+               : launch_batch_kernels<MX, PB, 2>(scenes, nscenes, units, tiles, smem, resident, L0, done, s);
+}
+
+template <int MX, int PB>
+int batch_resident_mx_pb(size_t smem) {
+    return smem > 113u * 1024u ? resident_of(bp_mixed_kernel<MX, PB, false, 1, true>, smem)
+                               : resident_of(bp_mixed_kernel<MX, PB, false, 2, true>, smem);
 }
 
 }  // namespace
@@ -421,6 +543,42 @@ int bp_mixed_resident(const TileConfig &tc, size_t smem) {
     SARBP_MIXED_CASE(1, 2)
     SARBP_MIXED_CASE(1, 1)
 #undef SARBP_MIXED_CASE
+    return 0;
+}
+
+// Tile shapes instantiated for batches; the batch autotuner times these.
+const TileConfig bp_batch_tiles[] = {{4, 8}, {4, 4}, {2, 8}, {2, 4}, {1, 8}, {1, 4}};
+const int bp_batch_tile_count = static_cast<int>(sizeof(bp_batch_tiles) / sizeof(bp_batch_tiles[0]));
+
+cudaError_t launch_bp_mixed_batch(const BatchScene *scenes, int nscenes, long long units, long long tiles,
+                                  const TileConfig &tc, size_t smem, int resident, void *partial,
+                                  unsigned long long *done, cudaStream_t s, int max_wsize) {
+    BpLaunch L0{};
+    L0.wsize = max_wsize;
+    L0.sk_partial = partial;
+#define SARBP_BATCH_CASE(MX_, PB_) \
+    if (tc.mx == MX_ && tc.pb == PB_)  \
+        return launch_batch_mx_pb<MX_, PB_>(scenes, nscenes, units, tiles, smem, resident, L0, done, s);
+    SARBP_BATCH_CASE(4, 8)
+    SARBP_BATCH_CASE(4, 4)
+    SARBP_BATCH_CASE(2, 8)
+    SARBP_BATCH_CASE(2, 4)
+    SARBP_BATCH_CASE(1, 8)
+    SARBP_BATCH_CASE(1, 4)
+#undef SARBP_BATCH_CASE
+    return cudaErrorInvalidValue;
+}
+
+int bp_mixed_batch_resident(const TileConfig &tc, size_t smem) {
+#define SARBP_BATCH_CASE(MX_, PB_) \
+    if (tc.mx == MX_ && tc.pb == PB_) return batch_resident_mx_pb<MX_, PB_>(smem);
+    SARBP_BATCH_CASE(4, 8)
+    SARBP_BATCH_CASE(4, 4)
+    SARBP_BATCH_CASE(2, 8)
+    SARBP_BATCH_CASE(2, 4)
+    SARBP_BATCH_CASE(1, 8)
+    SARBP_BATCH_CASE(1, 4)
+#undef SARBP_BATCH_CASE
     return 0;
 }
 

@@ -56,10 +56,11 @@ __device__ __forceinline__ long long sk_owner(long long u, long long units, long
     return c;
 }
 
-// Partial-sum slot of CTA c's segment of tile t: its first segment (the one
-// holding unit lo(c)) uses slot 2c, a later one slot 2c + 1.
-__device__ __forceinline__ long long sk_slot(long long c, long long t, const TileGrid &g, long long G) {
-    return sk_lo(c, g.units, G) >= t * g.stages ? 2 * c : 2 * c + 1;
+// Partial-sum slot of CTA c's segment of the tile whose first unit is
+// `first`: its first segment (the one holding unit lo(c)) uses slot 2c, a
+// later one slot 2c + 1.
+__device__ __forceinline__ long long sk_slot(long long c, long long first, long long units, long long G) {
+    return sk_lo(c, units, G) >= first ? 2 * c : 2 * c + 1;
 }
 
 // Pixel origin (row tx0, column ty0) and hypothesis-major slice zz of tile t.

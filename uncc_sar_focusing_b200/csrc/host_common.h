@@ -1,0 +1,143 @@
+// host_common.h -- host-side helpers shared by the plan (api.cu) and batch
+// (batch.cu) entry points: status mapping, device guard, descriptor checks,
+// grid axes, window geometry and the range-compression factors.
+#pragma once
+
+#include <cmath>
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <vector>
+
+#include "bp_common.cuh"
+#include "sarbp_internal.h"
+
+namespace sarbp {
+namespace host {
+
+inline int from_cuda(cudaError_t e) {
+    if (e == cudaSuccess) return SARBP_OK;
+    if (e == cudaErrorMemoryAllocation) return SARBP_ERR_OUT_OF_MEMORY;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return SARBP_ERR_NO_DEVICE;
+    return SARBP_ERR_CUDA;
+}
+
+inline int from_cufft(cufftResult r) {
+    if (r == CUFFT_SUCCESS) return SARBP_OK;
+    if (r == CUFFT_ALLOC_FAILED) return SARBP_ERR_OUT_OF_MEMORY;
+    return SARBP_ERR_CUFFT;
+}
+
+#define SARBP_TRY(call)                  \
+    do {                                 \
+        const int st_ = (call);          \
+        if (st_ != SARBP_OK) return st_; \
+    } while (0)
+
+#define SARBP_TRY_CUDA(call)                         \
+    do {                                             \
+        const cudaError_t e_ = (call);               \
+        if (e_ != cudaSuccess) {                     \
+            cudaGetLastError();                      \
+            return ::sarbp::host::from_cuda(e_);     \
+        }                                            \
+    } while (0)
+
+// Makes a device current for the duration of a call and restores the
+// caller's device afterwards.
+struct DeviceGuard {
+    int prev = -1;
+    bool changed = false;
+    cudaError_t status = cudaSuccess;
+    explicit DeviceGuard(int dev) {
+        status = cudaGetDevice(&prev);
+        if (status == cudaSuccess && prev != dev) {
+            status = cudaSetDevice(dev);
+            changed = status == cudaSuccess;
+        }
+    }
+    ~DeviceGuard() {
+        if (changed) cudaSetDevice(prev);
+    }
+};
+
+inline bool finite_nonneg(double v) { return std::isfinite(v) && v >= 0.0; }
+
+inline int validate_desc(const sarbp_plan_desc *d) {
+    if (!d) return SARBP_ERR_NULL_POINTER;
+    const sarbp_grid &g = d->grid;
+    if (d->num_range_samples < 1 || d->num_pulses < 1 || d->nfft < 2 || d->nfft < d->num_range_samples ||
+        d->nfft > (1 << 24))
+        return SARBP_ERR_INVALID_ARGUMENT;
+    if (!(std::isfinite(d->max_wr) && d->max_wr > 0.0)) return SARBP_ERR_INVALID_ARGUMENT;
+    if (g.nx < 1 || g.ny < 1 || g.nz < 1 || g.nx > (1 << 20) || g.ny > (1 << 20) || g.nz > 65535)
+        return SARBP_ERR_INVALID_ARGUMENT;
+    if (!(std::isfinite(g.x0) && std::isfinite(g.y0) && std::isfinite(g.z0) && finite_nonneg(g.wx) &&
+          finite_nonneg(g.wy) && finite_nonneg(g.wz)))
+        return SARBP_ERR_INVALID_ARGUMENT;
+    if (d->precision != SARBP_PRECISION_MIXED && d->precision != SARBP_PRECISION_FP64)
+        return SARBP_ERR_INVALID_ARGUMENT;
+    if (d->window != SARBP_WINDOW_NONE && d->window != SARBP_WINDOW_HAMMING) return SARBP_ERR_INVALID_ARGUMENT;
+    const double samples = static_cast<double>(d->num_pulses) * static_cast<double>(d->nfft);
+    if (samples > 4.0e9) return SARBP_ERR_UNSUPPORTED;
+    return SARBP_OK;
+}
+
+// First coordinate and step of a linspace axis of n points of width w
+// centred on c (cpuBackProjection.hpp:55-62).
+inline void axis(int n, double c, double w, double *lo, double *step) {
+    if (n > 1) {
+        *step = w / static_cast<double>(n - 1);
+        *lo = c - 0.5 * w;
+    } else {
+        *step = 0.0;
+        *lo = c;
+    }
+}
+
+// Range-bin window of a tile of (8 mx) x 64 pixels with steps dx, dy at
+// lambda bins per metre: W = ceil(lambda * half-diagonal) + 3 bins each side,
+// wsize = 2W + 2 pair entries; hd the half-diagonal in metres.
+inline void tile_window(double lambda, double dx, double dy, int mx, int *W, int *wsize, double *hd) {
+    const double hx = 0.5 * 8.0 * mx * dx, hy = 0.5 * 64.0 * dy;
+    *hd = std::sqrt(hx * hx + hy * hy);
+    *W = static_cast<int>(std::ceil(lambda * *hd)) + 3;
+    *wsize = 2 * (*W) + 2;
+}
+
+// Far-field test constants of the mixed kernel for a tile half-diagonal hd:
+// the remainder after the e (h + t hr) expansion is <= 0.625 hd^4 / Rc^3
+// metres; a pulse whose k times that exceeds 1e-7 revolutions takes the
+// exact path.
+inline void near_field_consts(double hd, double *near_hd16, double *near_coef) {
+    *near_hd16 = 16.0 * hd;
+    *near_coef = 0.625 * hd * hd * hd * hd / 1.0e-7;
+}
+
+// fac[k] = w_k / nfft * exp(+j 2 pi ((k s) mod nfft) / nfft), s = (nfft+1)/2,
+// interleaved re, im: taper (Hamming or none), the 1/nfft of the inverse FFT
+// and the fftshift as an input twiddle.
+inline std::vector<double> range_factors(const sarbp_plan_desc &d) {
+    const int K = d.num_range_samples, N = d.nfft;
+    const long long s = (N + 1) / 2;
+    std::vector<double> fac(2 * static_cast<size_t>(K));
+    for (int k = 0; k < K; ++k) {
+        double w = 1.0;
+        if (d.window == SARBP_WINDOW_HAMMING && K > 1)
+            w = 0.54 - 0.46 * std::cos(2.0 * M_PI * static_cast<double>(k) / static_cast<double>(K - 1));
+        const long long m = (static_cast<long long>(k) * s) % N;
+        const double ang = 2.0 * M_PI * static_cast<double>(m) / static_cast<double>(N);
+        fac[2 * k] = w / N * std::cos(ang);
+        fac[2 * k + 1] = w / N * std::sin(ang);
+    }
+    return fac;
+}
+
+inline int status_from_bits(unsigned bits) {
+    if (bits & ERRBIT_TIMEOUT) return SARBP_ERR_KERNEL_TIMEOUT;
+    if (bits & ERRBIT_NOT_FINITE) return SARBP_ERR_NOT_FINITE;
+    if (bits & ERRBIT_BOUNDS) return SARBP_ERR_KERNEL_BOUNDS;
+    return SARBP_OK;
+}
+
+}  // namespace host
+}  // namespace sarbp

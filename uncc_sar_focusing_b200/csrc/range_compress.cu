@@ -75,6 +75,47 @@ __global__ void rc_pairs_kernel(const C *__restrict__ X, E *__restrict__ pairs, 
     }
 }
 
+// Batch forms: scene blockIdx.y of the table, grid-stride over its elements.
+__global__ void rc_prep_batch_kernel(const BatchScene *__restrict__ scenes) {
+    const BatchScene &S = scenes[blockIdx.y];
+    const float2 *__restrict__ ph = static_cast<const float2 *>(S.ph);
+    const float2 *__restrict__ fac = static_cast<const float2 *>(S.fac);
+    float2 *__restrict__ out = static_cast<float2 *>(S.fft);
+    const int K = S.K, nfft = S.L.nfft;
+    const long long total = static_cast<long long>(S.L.np) * nfft;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long p = i / nfft;
+        const int k = static_cast<int>(i - p * nfft);
+        float2 v = make_float2(0.0f, 0.0f);
+        if (k < K) {
+            const float2 x = ph[p * K + k];
+            const float2 f = fac[k];
+            v.x = x.x * f.x - x.y * f.y;
+            v.y = x.x * f.y + x.y * f.x;
+        }
+        out[i] = v;
+    }
+}
+
+__global__ void rc_pairs_batch_kernel(const BatchScene *__restrict__ scenes) {
+    const BatchScene &S = scenes[blockIdx.y];
+    const float2 *__restrict__ X = static_cast<const float2 *>(S.fft);
+    float4 *__restrict__ pairs = static_cast<float4 *>(const_cast<void *>(S.L.pairs));
+    const int nfft = S.L.nfft, guard = S.L.guard;
+    const int per = nfft + 1;
+    const long long total = static_cast<long long>(S.L.np) * per;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long p = i / per;
+        const int b = static_cast<int>(i - p * per) - 1;
+        float2 v = make_float2(0.0f, 0.0f), vn = make_float2(0.0f, 0.0f);
+        if (b >= 0) v = X[p * nfft + b];
+        if (b + 1 < nfft) vn = X[p * nfft + b + 1];
+        make_pair(v, vn, pairs + p * S.row_stride + guard + b);
+    }
+}
+
 int grid_for(long long total) {
     long long blocks = (total + 255) / 256;
     const long long cap = 148LL * 16;
@@ -106,6 +147,18 @@ cudaError_t launch_rc_pairs(int precision, const void *fft_buf, void *pairs, int
     else
         rc_pairs_kernel<float2, float4><<<grid_for(total), 256, 0, s>>>(
             static_cast<const float2 *>(fft_buf), static_cast<float4 *>(pairs), nfft, total, row_stride, guard);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rc_prep_batch(const BatchScene *scenes, int nscenes, cudaStream_t s) {
+    if (nscenes < 1 || nscenes > 65535) return cudaErrorInvalidValue;
+    rc_prep_batch_kernel<<<dim3(128, nscenes), 256, 0, s>>>(scenes);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rc_pairs_batch(const BatchScene *scenes, int nscenes, cudaStream_t s) {
+    if (nscenes < 1 || nscenes > 65535) return cudaErrorInvalidValue;
+    rc_pairs_batch_kernel<<<dim3(128, nscenes), 256, 0, s>>>(scenes);
     return cudaGetLastError();
 }
 

@@ -39,6 +39,21 @@ struct BpLaunch {
     int sk_resident;          // CTAs of the kernel resident at once on the device (0: do not split)
 };
 
+// One scene of a batch (sarbp_batch_focus), in device memory.  The forward
+// kernel walks the units of all scenes, scene-major: scene s owns units
+// [unit_begin, unit_begin + its tiles x stages) and tiles
+// [tile_begin, tile_begin + its tiles) of the launch.
+struct BatchScene {
+    BpLaunch L;                 // the scene's backprojection (pairs, geometry, grid, image, window)
+    const void *ph;             // complex64 [np][K] phase history (device)
+    const void *fac;            // per-sample taper x scale x shift twiddle [K]
+    void *fft;                  // complex64 [np][nfft] FFT buffer
+    int K;
+    int pad0;
+    long long row_stride;       // pair entries per pulse row
+    long long unit_begin, tile_begin;
+};
+
 // Tile shape of the forward kernels (see bp_mixed.cu).
 struct TileConfig {
     int mx;   // rows per thread; tile = (8*mx) x 64 pixels, 256 threads
@@ -63,6 +78,18 @@ size_t bp_fp64_smem_bytes(const TileConfig &tc, int wsize);
 // launch with that many CTAs needs 2 * resident * (8 mx * 64) complex values
 // of sk_partial.
 int bp_mixed_resident(const TileConfig &tc, size_t smem);
+// Batch forward launch over `nscenes` scenes (table in device memory,
+// `units` = their total units, `tiles` = their total tiles): the split kernel
+// and, when tiles are split, the fix-up.  Completion time of each scene's
+// image (%globaltimer ns) goes to done[scene] (atomic max) when done != null.
+// max_wsize: the largest scene window (entries), the stage buffers' stride.
+// Instantiated for the tile shapes in bp_batch_tiles.
+cudaError_t launch_bp_mixed_batch(const BatchScene *scenes, int nscenes, long long units, long long tiles,
+                                  const TileConfig &tc, size_t smem, int resident, void *partial,
+                                  unsigned long long *done, cudaStream_t s, int max_wsize);
+int bp_mixed_batch_resident(const TileConfig &tc, size_t smem);
+extern const TileConfig bp_batch_tiles[];
+extern const int bp_batch_tile_count;
 int bp_fp64_resident(const TileConfig &tc, size_t smem);
 
 // Range compression kernels (range_compress.cu)
@@ -70,6 +97,10 @@ cudaError_t launch_rc_prep(int precision, const void *ph, const void *fac, void 
                            cudaStream_t s);
 cudaError_t launch_rc_pairs(int precision, const void *fft_buf, void *pairs, int nfft, int np, long long row_stride,
                             int guard, cudaStream_t s);
+// Range compression steps 1 and 3 for every scene of a batch in one launch
+// each (blockIdx.y = scene); the FFT in between runs per scene.
+cudaError_t launch_rc_prep_batch(const BatchScene *scenes, int nscenes, cudaStream_t s);
+cudaError_t launch_rc_pairs_batch(const BatchScene *scenes, int nscenes, cudaStream_t s);
 
 }  // namespace sarbp
 

@@ -282,6 +282,108 @@ class Plan:
         N.check(N.lib().sarbp_plan_check(self._h, s), "sarbp_plan_check")
 
 
+def _desc(K: int, num_pulses: int, nfft: int, max_wr: float, grid: Grid, precision: str, window, device: int):
+    d = N.PlanDesc()
+    d.num_range_samples = int(K)
+    d.num_pulses = int(num_pulses)
+    d.nfft = int(nfft)
+    d.max_wr = float(max_wr)
+    d.grid = N.Grid(grid.nx, grid.ny, grid.nz, grid.x0, grid.y0, grid.z0, grid.wx, grid.wy, grid.wz)
+    d.precision = _PRECISION[precision]
+    d.window = _WINDOW[window]
+    d.device = int(device)
+    return d
+
+
+class Batch:
+    """Independent scenes of uneven sizes focused together (sarbp_batch_*):
+    one backprojection launch over all scenes' tiles, replayed as a captured
+    CUDA graph.  Inputs and images are CUDA torch tensors; calls run on
+    torch's current stream."""
+
+    def __init__(self, scenes, device: int = -1):
+        self.grids = [sc.grid for sc in scenes]
+        self.K = [sc.num_range_samples for sc in scenes]
+        descs = (N.PlanDesc * len(scenes))(*[
+            _desc(sc.num_range_samples, sc.num_pulses, sc.nfft, sc.max_wr, sc.grid, "mixed", sc.window, device)
+            for sc in scenes])
+        h = ctypes.c_void_p()
+        N.check(N.lib().sarbp_batch_create(descs, len(scenes), ctypes.byref(h)), "sarbp_batch_create")
+        self._h = h
+        self.n = len(scenes)
+        self._keep = None
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            N.lib().sarbp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def new_images(self, device="cuda"):
+        import torch
+
+        return [torch.zeros((g.nz, g.nx, g.ny), dtype=torch.complex64, device=device) for g in self.grids]
+
+    def _args(self, apertures, images):
+        if len(apertures) != self.n or len(images) != self.n:
+            raise ValueError(f"need {self.n} apertures and images")
+        aps = (N.Aperture * self.n)()
+        keep = []
+        for i, (ap, img) in enumerate(zip(apertures, images)):
+            ph, ax, ay, az, r0, f0 = ap
+            n = int(ax.shape[0])
+            pp, pmem, pk = _ptr(ph, np.complex64, n * self.K[i])
+            gp = [_ptr(v, np.float64, n) for v in (ax, ay, az, r0, f0)]
+            ip, imem, ik = _ptr(img, np.complex64, int(np.prod(img.shape)))
+            if pmem != N.MEMORY_DEVICE or imem != N.MEMORY_DEVICE or any(m != N.MEMORY_DEVICE for _, m, _ in gp):
+                raise ValueError("batch inputs and images must be CUDA tensors")
+            aps[i] = N.Aperture(pp, pmem, N.Geometry(gp[0][0], gp[1][0], gp[2][0], gp[3][0], gp[4][0], n,
+                                                     N.MEMORY_DEVICE))
+            keep.append((pk, ik, [k for _, _, k in gp]))
+        imgs = (ctypes.c_void_p * self.n)(*[ctypes.c_void_p(img.data_ptr()) for img in images])
+        return aps, imgs, keep
+
+    def focus(self, apertures, images) -> None:
+        """apertures: per scene (phase_history [Np, K] complex64, ant_x,
+        ant_y, ant_z, slant_range, start_freq [Np] float64), CUDA tensors;
+        images: per scene complex64 [nz, nx, ny] CUDA tensors."""
+        aps, imgs, keep = self._args(apertures, images)
+        st = N.lib().sarbp_batch_focus(self._h, aps, imgs, _stream(images[0]))
+        N.check(st, "sarbp_batch_focus")
+        self._keep = keep
+
+    def wait(self):
+        """Wait for the last focus; per-image completion times (ms after the
+        call's start, GPU clock) as a numpy array."""
+        ms = (ctypes.c_double * self.n)()
+        N.check(N.lib().sarbp_batch_wait(self._h, ms), "sarbp_batch_wait")
+        return np.array(ms[:], dtype=np.float64)
+
+    def autotune(self, apertures, images) -> float:
+        aps, imgs, keep = self._args(apertures, images)
+        best = ctypes.c_double()
+        st = N.lib().sarbp_batch_autotune(self._h, aps, imgs, _stream(images[0]), ctypes.byref(best))
+        N.check(st, "sarbp_batch_autotune")
+        return float(best.value)
+
+    @property
+    def info(self) -> dict:
+        v = N.BatchInfo()
+        N.check(N.lib().sarbp_batch_get_info(self._h, ctypes.byref(v)), "sarbp_batch_get_info")
+        return {f: getattr(v, f) for f, _ in N.BatchInfo._fields_ if f != "reserved"}
+
+
 def focus_scene(scene: Scene, precision: str = "mixed") -> np.ndarray:
     """Focus a scene through host buffers (sarbp_focus on host memory)."""
     with Plan.for_scene(scene, precision) as plan:
