@@ -60,6 +60,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-autofocus", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-configuration section")
     ap.add_argument("--grid-seconds", type=float, default=20.0, help="bound on the grid-search baseline")
     ap.add_argument("--profile", action="store_true",
                     help="one warm-up and one focus step of the workload, nothing else (for ncu captures)")
@@ -293,6 +294,121 @@ def autofocus_section(dev, grid_seconds: float):
     }
 
 
+def batched_section(dev, steps: int):
+    """Batched configuration: (a) 256 motion hypotheses (seeded perturbations
+    of the autofocus scene's true cubic coefficients, 5 cm per coefficient) x
+    a 512^2 image from one 1024 x 512 phase history, one launch
+    (sarbp_backproject_hypotheses); (b) 64 independent point-target scenes of
+    seeded uniform sizes (128^2-1024^2 pixels at 0.1 m, 256-2048 pulses of
+    512 samples, 5-500 scatterers) focused as one batch (sarbp_batch_*): range
+    compression and ONE backprojection launch over all scenes' tiles, a
+    captured CUDA graph replayed per call, tile shape autotuned; throughput,
+    per-image completion latency p50/p99 (GPU clock, from the call's start),
+    and the same scenes focused one plan at a time beside it."""
+    import numpy as np
+    import torch
+
+    from uncc_sar_focusing_b200 import autofocus as AF
+    from uncc_sar_focusing_b200 import focusing
+    from uncc_sar_focusing_b200 import scenes as S
+
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, n):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(n):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / n
+
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    out = {}
+    # (a) hypotheses
+    sc = S.motion_error_scene(device=dev)
+    torch.cuda.empty_cache()
+    H = 256
+    ax, ay, az, r0, f0 = (d(v) for v in (sc.ant_x, sc.ant_y, sc.ant_z, sc.slant_range, sc.start_freq))
+    motion = AF.CubicMotion(ax, ay, az)
+    rng = np.random.default_rng(5)
+    theta = torch.as_tensor(sc.true_cubic[None] + rng.normal(0.0, 0.05, size=(H, 3, 4)), device=dev)
+    tracks = torch.stack([motion.track(theta[h]) for h in range(H)])  # [H, 3, Np]
+    hx, hy, hz = (tracks[:, i].contiguous() for i in range(3))
+    hr0 = r0.expand(H, -1).contiguous()
+    hf0 = f0.expand(H, -1).contiguous()
+    with focusing.Plan.for_scene(sc, "mixed", device=torch.cuda.current_device()) as plan:
+        plan.range_compress(d(sc.phase_history))
+        imgs = torch.empty((H, 1, sc.grid.nx, sc.grid.ny), dtype=torch.complex64, device=dev)
+        step = lambda: plan.backproject_hypotheses(hx, hy, hz, hr0, hf0, out=imgs)  # noqa: E731
+        step()
+        plan.check()
+        ms = timed(step, max(2, steps // 2))
+        plan.check()
+    pp = H * sc.grid.npix * sc.num_pulses
+    out["hypotheses"] = {"workload": f"{H} hypotheses x {sc.grid.nx}x{sc.grid.ny} image x {sc.num_pulses} pulses "
+                                     f"x {sc.num_range_samples} samples, one launch",
+                         "pixel_pulses": pp, "ms": ms, "value": pp / (ms * 1e-3), "unit": UNIT}
+    del imgs, tracks, hx, hy, hz, hr0, hf0
+    torch.cuda.empty_cache()
+
+    # (b) uneven scenes
+    rng = np.random.default_rng(55)
+    scenes = []
+    for i in range(64):
+        n = int(rng.integers(128, 1025))
+        npulse = int(rng.integers(256, 2049))
+        nt = int(rng.integers(5, 501))
+        scenes.append(S.point_target_scene(K=512, Np=npulse, n=n, spacing=0.1, n_targets=nt, nfft=4096,
+                                           seed=100 + i, extent=0.08 * n, device=dev))
+    args = [tuple(d(getattr(s_, a)) for a in ("phase_history", "ant_x", "ant_y", "ant_z", "slant_range",
+                                              "start_freq")) for s_ in scenes]
+    pp_b = sum(s_.pixel_pulses for s_ in scenes)
+    with focusing.Batch(scenes, device=torch.cuda.current_device()) as batch:
+        default_info = batch.info
+        imgs = batch.new_images(dev)
+        t0 = time.perf_counter()
+        best_ms = batch.autotune(args, imgs)
+        tune_s = time.perf_counter() - t0
+        batch.focus(args, imgs)
+        batch.wait()
+        ms_b = timed(lambda: batch.focus(args, imgs), max(3, steps // 2))
+        lat = batch.wait()
+        info = batch.info
+        batch_img0 = imgs[0].clone()
+    # the same scenes, one plan and one focus call each
+    plans = [focusing.Plan.for_scene(s_, "mixed", device=torch.cuda.current_device()) for s_ in scenes]
+    seq_imgs = [p.new_image(dev) for p in plans]
+    seq = lambda: [p.focus(*a, out=o) for p, a, o in zip(plans, args, seq_imgs)]  # noqa: E731
+    seq()
+    ms_seq = timed(seq, 2)
+    for p in plans:
+        p.check()
+    rel = float((seq_imgs[0] - batch_img0).abs().pow(2).sum().sqrt() / seq_imgs[0].abs().pow(2).sum().sqrt())
+    for p in plans:
+        p.close()
+    del seq_imgs, plans, imgs
+    torch.cuda.empty_cache()
+    out["uneven_scenes"] = {
+        "workload": "64 point-target scenes, seeded uniform sizes 128^2-1024^2 pixels at 0.1 m, 256-2048 pulses "
+                    "x 512 samples (Nfft 4096), 5-500 scatterers; one batch call = range compression + one "
+                    "backprojection launch over all scenes, CUDA graph replay",
+        "pixel_pulses": pp_b, "ms": ms_b, "value": pp_b / (ms_b * 1e-3), "unit": UNIT,
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "max": float(lat.max()), "of": "per-image completion after the call's start, GPU clock"},
+        "graph": bool(info["graph"]),
+        "schedule": "one CTA per tile, scene order" if info["per_tile"] else "units split over resident CTAs",
+        "autotune": {"tile_rows": 8 * info["tile_mx"], "stage_pulses": info["stage_pulses"],
+                     "default_tile_rows": 8 * default_info["tile_mx"],
+                     "default_stage_pulses": default_info["stage_pulses"], "best_ms": best_ms,
+                     "seconds": tune_s},
+        "sequential_plans": {"ms": ms_seq, "value": pp_b / (ms_seq * 1e-3),
+                             "batch_speedup": ms_seq / ms_b, "rel_l2_scene0_batch_vs_plan": rel},
+    }
+    return out
+
+
 def profiled_traffic(config: str):
     """DRAM bytes per backprojection launch from the committed ncu summary of
     this workload (profiles/), or None."""
@@ -492,6 +608,8 @@ def gpu_arm(args):
         }
         if world == 1 and not args.no_autofocus:
             line["autofocus"] = autofocus_section(dev, args.grid_seconds)
+        if world == 1 and not args.no_batched:
+            line["batched"] = batched_section(dev, args.steps)
         traffic = profiled_traffic(args.config)
         if traffic is not None:
             line["roofline"]["traffic"] = traffic

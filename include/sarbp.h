@@ -248,7 +248,12 @@ SARBP_API int sarbp_focus_wait(sarbp_plan *plan, unsigned long long ticket);
  * stores each image's completion time in ms after the call's start, from the
  * GPU clock.  sarbp_batch_autotune times every instantiated tile shape on
  * the given inputs (each run focuses them), keeps the fastest and returns
- * its time per batch. */
+ * its time per batch.  Two schedules exist for the backprojection launch:
+ * the units of all scenes split evenly over the resident CTAs (every scene
+ * completes near the end of the launch), or one CTA per tile in scene order
+ * (scenes complete one after another; a tail when few tiles are left).  The
+ * default is the split for batches of fewer than four waves of tiles, else
+ * one CTA per tile; the autotuner times both with every tile shape. */
 typedef struct sarbp_batch sarbp_batch;
 typedef struct sarbp_batch_info {
     int num_scenes;
@@ -261,7 +266,9 @@ typedef struct sarbp_batch_info {
     long long units;        /* (tile, stage) units of the last call */
     long long smem_bytes;
     long long workspace_bytes;
-    int reserved[4];
+    int per_tile;           /* 1: one CTA per tile in scene order (scenes finish one after
+                               another); 0: units split evenly over the resident CTAs */
+    int reserved[3];
 } sarbp_batch_info;
 SARBP_API int sarbp_batch_create(const sarbp_plan_desc *descs, int num_scenes, sarbp_batch **batch);
 SARBP_API int sarbp_batch_destroy(sarbp_batch *batch);
@@ -271,6 +278,8 @@ SARBP_API int sarbp_batch_wait(sarbp_batch *batch, double *image_ms);
 SARBP_API int sarbp_batch_autotune(sarbp_batch *batch, const sarbp_aperture *apertures, void *const *images,
                                    void *stream, double *best_ms);
 SARBP_API int sarbp_batch_get_info(const sarbp_batch *batch, sarbp_batch_info *info);
+/* Force a schedule: 1 one CTA per tile, 0 split, -1 automatic (default). */
+SARBP_API int sarbp_batch_set_schedule(sarbp_batch *batch, int per_tile);
 
 /* One call, no plan kept: create, focus, destroy (host or device buffers). */
 SARBP_API int sarbp_focus_image(const sarbp_plan_desc *desc, const sarbp_aperture *aperture, void *image,

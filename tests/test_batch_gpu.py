@@ -78,6 +78,20 @@ def test_uneven_batch_matches_oracle_and_single_plans(F):
     torch.cuda.synchronize()
 
 
+@pytest.mark.parametrize("per_tile", [False, True])
+def test_both_schedules(F, per_tile):
+    scenes = [make(s) for s in SHAPES]
+    with F.Batch(scenes) as batch:
+        batch.set_schedule(per_tile)
+        imgs = batch.new_images()
+        batch.focus([dev_args(sc) for sc in scenes], imgs)
+        ms = batch.wait()
+        assert batch.info["per_tile"] == int(per_tile)
+    assert np.isfinite(ms).all() and (ms > 0).all()
+    for sc, img in zip(scenes, imgs):
+        assert O.rel_l2(img.cpu().numpy(), single(F, sc)) < 1e-5
+
+
 def test_graph_replay_with_new_buffers_and_pulse_counts(F):
     scenes = [make(s) for s in SHAPES[:3]]
     others = [make(s[:-1] + (s[-1] + 10,)) for s in SHAPES[:3]]

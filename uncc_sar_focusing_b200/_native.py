@@ -40,7 +40,7 @@ EXPORTED = (
     "sarbp_focus", "sarbp_focus_image", "sarbp_plan_check", "sarbp_backproject_noalloc",
     "sarbp_backproject_adjoint", "sarbp_backproject_hypotheses", "sarbp_focus_submit", "sarbp_focus_wait", "sarbp_plan_get_info",
     "sarbp_batch_create", "sarbp_batch_destroy", "sarbp_batch_focus", "sarbp_batch_wait", "sarbp_batch_autotune",
-    "sarbp_batch_get_info",
+    "sarbp_batch_get_info", "sarbp_batch_set_schedule",
 )
 
 
@@ -66,7 +66,7 @@ class BatchInfo(ctypes.Structure):
     _fields_ = [("num_scenes", ctypes.c_int), ("tile_mx", ctypes.c_int), ("stage_pulses", ctypes.c_int),
                 ("max_window_bins", ctypes.c_int), ("resident_ctas", ctypes.c_int), ("graph", ctypes.c_int),
                 ("tiles", ctypes.c_longlong), ("units", ctypes.c_longlong), ("smem_bytes", ctypes.c_longlong),
-                ("workspace_bytes", ctypes.c_longlong), ("reserved", ctypes.c_int * 4)]
+                ("workspace_bytes", ctypes.c_longlong), ("per_tile", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
 
 
 class Geometry(ctypes.Structure):
@@ -114,6 +114,7 @@ def lib():
         L.sarbp_batch_wait.argtypes = [vp, P(ctypes.c_double)]
         L.sarbp_batch_autotune.argtypes = [vp, P(Aperture), P(vp), vp, P(ctypes.c_double)]
         L.sarbp_batch_get_info.argtypes = [vp, P(BatchInfo)]
+        L.sarbp_batch_set_schedule.argtypes = [vp, i]
         for name in EXPORTED:
             if name != "sarbp_status_string":
                 getattr(L, name).restype = i

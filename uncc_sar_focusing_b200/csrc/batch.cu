@@ -39,6 +39,7 @@ struct sarbp_batch {
     TileConfig tile{0, 0};
     size_t smem = 0;
     int resident = 0, max_wsize = 0;
+    int per_tile = -1;  // -1: choose per call (split below four waves of tiles)
     std::vector<int> W, wsize;
     std::vector<double> near_hd16, near_coef;
     // per call
@@ -224,6 +225,10 @@ int fill_table(sarbp_batch *b, const sarbp_aperture *aps, void *const *images) {
     return SARBP_OK;
 }
 
+bool per_tile_now(const sarbp_batch *b) {
+    return b->per_tile >= 0 ? b->per_tile != 0 : b->tiles >= 4LL * b->resident;
+}
+
 // The work of one call on stream s (captured into the graph, or run eagerly).
 int enqueue(sarbp_batch *b, cudaStream_t s) {
     const int n = b->n;
@@ -241,7 +246,7 @@ int enqueue(sarbp_batch *b, cudaStream_t s) {
     }
     SARBP_TRY_CUDA(launch_rc_pairs_batch(b->d_table, n, s));
     SARBP_TRY_CUDA(launch_bp_mixed_batch(b->d_table, n, b->units, b->tiles, b->tile, b->smem, b->resident,
-                                         b->d_partial, b->d_times, s, b->max_wsize));
+                                         b->d_partial, b->d_times, s, b->max_wsize, per_tile_now(b)));
     SARBP_TRY_CUDA(cudaMemcpyAsync(b->h_times, b->d_times, (n + 1) * sizeof(unsigned long long),
                                    cudaMemcpyDeviceToHost, s));
     SARBP_TRY_CUDA(cudaMemcpyAsync(b->h_err, b->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
@@ -448,7 +453,9 @@ int sarbp_batch_autotune(sarbp_batch *b, const sarbp_aperture *aps, void *const 
     SARBP_TRY_CUDA(guard.status);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const TileConfig start = b->tile;
+    const int start_sched = b->per_tile;
     TileConfig best{0, 0};
+    int best_sched = 0;
     double best_t = 0.0;
     cudaEvent_t e0, e1;
     SARBP_TRY_CUDA(cudaEventCreate(&e0));
@@ -458,12 +465,13 @@ int sarbp_batch_autotune(sarbp_batch *b, const sarbp_aperture *aps, void *const 
         return SARBP_ERR_CUDA;
     }
     int st = SARBP_OK;
-    for (int c = 0; c < bp_batch_tile_count && st == SARBP_OK; ++c) {
+    for (int c = 0; c < 2 * bp_batch_tile_count && st == SARBP_OK; ++c) {
         if (b->launched && cudaEventSynchronize(b->done_ev) != cudaSuccess) {
             st = SARBP_ERR_CUDA;
             break;
         }
-        if (!configure(b, bp_batch_tiles[c])) continue;
+        if (!configure(b, bp_batch_tiles[c / 2])) continue;
+        b->per_tile = c & 1;
         // two warm-up calls (the first captures the graph), then three timed
         for (int w = 0; w < 2 && st == SARBP_OK; ++w) st = focus_impl(b, aps, images, s);
         if (st == SARBP_OK) st = wait_impl(b, nullptr);
@@ -476,7 +484,8 @@ int sarbp_batch_autotune(sarbp_batch *b, const sarbp_aperture *aps, void *const 
             st = SARBP_ERR_CUDA;
         if (st == SARBP_OK) st = wait_impl(b, nullptr);
         if (st == SARBP_OK && (!best.mx || ms / 3.0 < best_t)) {
-            best = bp_batch_tiles[c];
+            best = bp_batch_tiles[c / 2];
+            best_sched = c & 1;
             best_t = ms / 3.0;
         }
     }
@@ -486,8 +495,20 @@ int sarbp_batch_autotune(sarbp_batch *b, const sarbp_aperture *aps, void *const 
     if (b->launched) cudaEventSynchronize(b->done_ev);
     if (st == SARBP_OK && !best.mx) st = SARBP_ERR_UNSUPPORTED;
     if (!configure(b, st == SARBP_OK ? best : start) && st == SARBP_OK) st = SARBP_ERR_CUDA;
+    b->per_tile = st == SARBP_OK ? best_sched : start_sched;
     if (st == SARBP_OK && best_ms) *best_ms = best_t;
     return st;
+}
+
+int sarbp_batch_set_schedule(sarbp_batch *b, int per_tile) {
+    if (!b) return SARBP_ERR_NULL_POINTER;
+    if (per_tile < -1 || per_tile > 1) return SARBP_ERR_INVALID_ARGUMENT;
+    DeviceGuard guard(b->device);
+    SARBP_TRY_CUDA(guard.status);
+    if (b->launched) SARBP_TRY_CUDA(cudaEventSynchronize(b->done_ev));
+    b->per_tile = per_tile;
+    drop_graph(b);
+    return SARBP_OK;
 }
 
 int sarbp_batch_get_info(const sarbp_batch *b, sarbp_batch_info *info) {
@@ -503,6 +524,7 @@ int sarbp_batch_get_info(const sarbp_batch *b, sarbp_batch_info *info) {
     info->units = b->units;
     info->smem_bytes = static_cast<long long>(b->smem);
     info->workspace_bytes = static_cast<long long>(b->bytes);
+    info->per_tile = per_tile_now(b) ? 1 : 0;
     return SARBP_OK;
 }
 

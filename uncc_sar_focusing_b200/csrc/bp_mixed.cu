@@ -223,7 +223,7 @@ struct SceneCursor {
 template <int MX, int PB, bool CHECKED, int MINB, bool BATCH>
 __global__ void __launch_bounds__(kThreads, MINB)
     bp_mixed_kernel(const __grid_constant__ BpLaunch L0, const BatchScene *__restrict__ scenes, int nscenes,
-                    long long batch_units, unsigned long long *__restrict__ done) {
+                    long long batch_units, unsigned long long *__restrict__ done, int tile_mode) {
     constexpr int TX = 8 * MX;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
@@ -237,8 +237,20 @@ __global__ void __launch_bounds__(kThreads, MINB)
     // this CTA's units [lo, lo + n) of the launch's (tile, stage) units
     const long long U = BATCH ? batch_units : tile_grid(L0, TX, PB).units;
     const long long G = gridDim.x;
-    const long long lo = sk_lo(blockIdx.x, U, G);
-    const int n = static_cast<int>(sk_lo(blockIdx.x + 1, U, G) - lo);
+    long long lo = sk_lo(blockIdx.x, U, G);
+    int n = static_cast<int>(sk_lo(blockIdx.x + 1, U, G) - lo);
+    if (BATCH && tile_mode) {
+        // one CTA per tile of the batch, in scene order: CTA t takes tile t's stages
+        int a = 0, z = nscenes - 1;  // last scene with tile_begin <= t
+        while (a < z) {
+            const int m = (a + z + 1) >> 1;
+            if (scenes[m].tile_begin <= static_cast<long long>(blockIdx.x)) a = m;
+            else z = m - 1;
+        }
+        const int S = tile_grid(scenes[a].L, TX, PB).stages;
+        lo = scenes[a].unit_begin + (static_cast<long long>(blockIdx.x) - scenes[a].tile_begin) * S;
+        n = S;
+    }
     if (n <= 0) return;
     const int i0 = warp - TX / 2;
     const int j0 = 2 * lane - kTY / 2;
@@ -448,7 +460,7 @@ cudaError_t launch_kernels(const BpLaunch &L, size_t smem, cudaStream_t s) {
         if (2 * g * TX * kTY * static_cast<long long>(sizeof(float2)) <= L.sk_slot_bytes) G = g;
     }
     if (G > 0x7fffffffLL) return cudaErrorInvalidValue;
-    kern<<<static_cast<unsigned>(G), kThreads, smem, s>>>(L, nullptr, 0, 0, nullptr);
+    kern<<<static_cast<unsigned>(G), kThreads, smem, s>>>(L, nullptr, 0, 0, nullptr, 0);
     e = cudaGetLastError();
     if (e != cudaSuccess || G == tg.tiles) return e;
     bp_sk_fixup_kernel<MX, PB, false>
@@ -489,13 +501,19 @@ int resident_mx_pb(size_t smem) {
 template <int MX, int PB, int MINB>
 cudaError_t launch_batch_kernels(const BatchScene *scenes, int nscenes, long long units, long long tiles,
                                  size_t smem, int resident, const BpLaunch &L0, unsigned long long *done,
-                                 cudaStream_t s) {
+                                 bool per_tile, cudaStream_t s) {
     auto kern = bp_mixed_kernel<MX, PB, false, MINB, true>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
+    if (tiles < 1 || tiles > 0x7fffffffLL) return cudaErrorInvalidValue;
+    if (per_tile) {
+        // one CTA per tile: no partial sums, scenes finish in order
+        kern<<<static_cast<unsigned>(tiles), kThreads, smem, s>>>(L0, scenes, nscenes, units, done, 1);
+        return cudaGetLastError();
+    }
     const long long G = resident < units ? resident : units;
-    if (G < 1 || G > 0x7fffffffLL || tiles > 0x7fffffffLL) return cudaErrorInvalidValue;
-    kern<<<static_cast<unsigned>(G), kThreads, smem, s>>>(L0, scenes, nscenes, units, done);
+    if (G < 1 || G > 0x7fffffffLL) return cudaErrorInvalidValue;
+    kern<<<static_cast<unsigned>(G), kThreads, smem, s>>>(L0, scenes, nscenes, units, done, 0);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     bp_sk_fixup_kernel<MX, PB, true>
@@ -505,10 +523,12 @@ cudaError_t launch_batch_kernels(const BatchScene *scenes, int nscenes, long lon
 
 template <int MX, int PB>
 cudaError_t launch_batch_mx_pb(const BatchScene *scenes, int nscenes, long long units, long long tiles, size_t smem,
-                               int resident, const BpLaunch &L0, unsigned long long *done, cudaStream_t s) {
+                               int resident, const BpLaunch &L0, unsigned long long *done, bool per_tile,
+                               cudaStream_t s) {
     return smem > 113u * 1024u
-               ? launch_batch_kernels<MX, PB, 1>(scenes, nscenes, units, tiles, smem, resident, L0, done, s)
-               : launch_batch_kernels<MX, PB, 2>(scenes, nscenes, units, tiles, smem, resident, L0, done, s);
+               ? launch_batch_kernels<MX, PB, 1>(scenes, nscenes, units, tiles, smem, resident, L0, done, per_tile, s)
+               : launch_batch_kernels<MX, PB, 2>(scenes, nscenes, units, tiles, smem, resident, L0, done, per_tile,
+                                                 s);
 }
 
 template <int MX, int PB>
@@ -552,13 +572,13 @@ const int bp_batch_tile_count = static_cast<int>(sizeof(bp_batch_tiles) / sizeof
 
 cudaError_t launch_bp_mixed_batch(const BatchScene *scenes, int nscenes, long long units, long long tiles,
                                   const TileConfig &tc, size_t smem, int resident, void *partial,
-                                  unsigned long long *done, cudaStream_t s, int max_wsize) {
+                                  unsigned long long *done, cudaStream_t s, int max_wsize, bool per_tile) {
     BpLaunch L0{};
     L0.wsize = max_wsize;
     L0.sk_partial = partial;
 #define SARBP_BATCH_CASE(MX_, PB_) \
     if (tc.mx == MX_ && tc.pb == PB_)  \
-        return launch_batch_mx_pb<MX_, PB_>(scenes, nscenes, units, tiles, smem, resident, L0, done, s);
+        return launch_batch_mx_pb<MX_, PB_>(scenes, nscenes, units, tiles, smem, resident, L0, done, per_tile, s);
     SARBP_BATCH_CASE(4, 8)
     SARBP_BATCH_CASE(4, 4)
     SARBP_BATCH_CASE(2, 8)

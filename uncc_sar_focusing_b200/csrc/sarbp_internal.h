@@ -83,10 +83,12 @@ int bp_mixed_resident(const TileConfig &tc, size_t smem);
 // and, when tiles are split, the fix-up.  Completion time of each scene's
 // image (%globaltimer ns) goes to done[scene] (atomic max) when done != null.
 // max_wsize: the largest scene window (entries), the stage buffers' stride.
+// per_tile: one CTA per tile in scene order instead of the even split (no
+// partial sums; scenes complete one after another).
 // Instantiated for the tile shapes in bp_batch_tiles.
 cudaError_t launch_bp_mixed_batch(const BatchScene *scenes, int nscenes, long long units, long long tiles,
                                   const TileConfig &tc, size_t smem, int resident, void *partial,
-                                  unsigned long long *done, cudaStream_t s, int max_wsize);
+                                  unsigned long long *done, cudaStream_t s, int max_wsize, bool per_tile);
 int bp_mixed_batch_resident(const TileConfig &tc, size_t smem);
 extern const TileConfig bp_batch_tiles[];
 extern const int bp_batch_tile_count;

@@ -377,6 +377,12 @@ class Batch:
         N.check(st, "sarbp_batch_autotune")
         return float(best.value)
 
+    def set_schedule(self, per_tile: Optional[bool]) -> None:
+        """True: one CTA per tile in scene order; False: units split over the
+        resident CTAs; None: automatic."""
+        v = -1 if per_tile is None else int(bool(per_tile))
+        N.check(N.lib().sarbp_batch_set_schedule(self._h, v), "sarbp_batch_set_schedule")
+
     @property
     def info(self) -> dict:
         v = N.BatchInfo()
