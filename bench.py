@@ -61,6 +61,7 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-autofocus", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-configuration section")
+    ap.add_argument("--no-volumetric", action="store_true", help="skip the volumetric-configuration section")
     ap.add_argument("--grid-seconds", type=float, default=20.0, help="bound on the grid-search baseline")
     ap.add_argument("--profile", action="store_true",
                     help="one warm-up and one focus step of the workload, nothing else (for ncu captures)")
@@ -409,6 +410,66 @@ def batched_section(dev, steps: int):
     return out
 
 
+def volumetric_section(dev, steps: int):
+    """Volumetric configuration at full size: 8 circular passes at elevations
+    30.0-31.4 deg (0.2 deg steps), 360 deg of azimuth, 1024 pulses per pass x
+    512 samples (9.6 GHz / 600 MHz, 10 km), 500 Rayleigh scatterers on random
+    planar facets in a 10 m cube, 256 x 256 x 64 voxels (3.44e10 voxel-pulses
+    per focus): mixed and FP64 throughput, and the relative L2 of every z-slice
+    of the mixed image against the FP64 path."""
+    import numpy as np
+    import torch
+
+    from uncc_sar_focusing_b200 import focusing
+    from uncc_sar_focusing_b200 import scenes as S
+
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, n):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(n):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / n
+
+    sc = S.volumetric_scene(device=dev)
+    torch.cuda.empty_cache()
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    ph = d(sc.phase_history)
+    geo = [d(v) for v in (sc.ant_x, sc.ant_y, sc.ant_z, sc.slant_range, sc.start_freq)]
+    dv = torch.cuda.current_device()
+    with focusing.Plan.for_scene(sc, "mixed", device=dv) as plan:
+        img = plan.new_image(dev)
+        plan.focus(ph, *geo, out=img)
+        plan.check()
+        ms = timed(lambda: plan.focus(ph, *geo, out=img), max(3, steps // 2))
+        plan.check()
+    with focusing.Plan.for_scene(sc, "fp64", device=dv) as plan64:
+        img64 = plan64.new_image(dev)
+        plan64.focus(ph, *geo, out=img64)
+        plan64.check()
+        ms64 = timed(lambda: plan64.focus(ph, *geo, out=img64), 2)
+        plan64.check()
+    diff = (img.to(torch.complex128) - img64).abs().pow(2).sum(dim=(1, 2)).sqrt()
+    per_slice = (diff / img64.abs().pow(2).sum(dim=(1, 2)).sqrt()).cpu().numpy()
+    total = float(diff.pow(2).sum().sqrt() / img64.abs().pow(2).sum().sqrt())
+    pp = sc.pixel_pulses
+    del img, img64
+    torch.cuda.empty_cache()
+    return {
+        "workload": "volumetric: 8 passes x 1024 pulses x 512 samples, 360 deg azimuth, el 30.0-31.4 deg, "
+                    "500 Rayleigh scatterers on facets in a 10 m cube, 256x256x64 voxels, Nfft 4096",
+        "voxel_pulses": pp, "ms": ms, "value": pp / (ms * 1e-3), "unit": UNIT,
+        "fp64": {"ms": ms64, "value": pp / (ms64 * 1e-3), "mixed_speedup": ms64 / ms},
+        "rel_l2_vs_fp64": {"total": total, "slice_min": float(per_slice.min()),
+                           "slice_median": float(np.median(per_slice)), "slice_max": float(per_slice.max()),
+                           "tolerance": 1e-4},
+    }
+
+
 def profiled_traffic(config: str):
     """DRAM bytes per backprojection launch from the committed ncu summary of
     this workload (profiles/), or None."""
@@ -610,6 +671,8 @@ def gpu_arm(args):
             line["autofocus"] = autofocus_section(dev, args.grid_seconds)
         if world == 1 and not args.no_batched:
             line["batched"] = batched_section(dev, args.steps)
+        if world == 1 and not args.no_volumetric:
+            line["volumetric"] = volumetric_section(dev, args.steps)
         traffic = profiled_traffic(args.config)
         if traffic is not None:
             line["roofline"]["traffic"] = traffic

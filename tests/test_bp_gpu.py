@@ -185,3 +185,18 @@ def test_large_config_sampled_pixels(F):
     assert O.rel_l2(got, want) < MIXED_TOL
     assert np.isfinite(img).all()
     torch.cuda.empty_cache()
+
+
+def test_volumetric_config_per_slice(F):
+    """Volumetric configuration (8 circular passes at 30.0-31.4 deg, 360 deg of
+    azimuth, scatterers on planar facets in a 10 m cube), reduced to 8 x 64
+    pulses x 128 samples and 48 x 48 x 12 voxels so the FP64 oracle runs in
+    seconds: every z-slice within 1e-4 of the oracle."""
+    sc = S.volumetric_scene(K=128, pulses_per_pass=64, nx=48, ny=48, nz=12, n_targets=120, seed=7)
+    want = O.focus_fp64(sc)
+    got = F.focus_scene(sc, "mixed")
+    assert got.shape == (12, 48, 48)
+    per_slice = [O.rel_l2(got[z], want[z]) for z in range(12)]
+    assert max(per_slice) < MIXED_TOL, per_slice
+    got64 = F.focus_scene(sc, "fp64")
+    assert O.rel_l2(got64, want) < FP64_TOL
