@@ -66,6 +66,8 @@ def parse_args():
     ap.add_argument("--profile", action="store_true",
                     help="one warm-up and one focus step of the workload, nothing else (for ncu captures)")
     ap.add_argument("--pulses", type=int, default=0, help="use only the first N pulses (profiling)")
+    ap.add_argument("--profile-precision", choices=["mixed", "fp64"], default="mixed",
+                    help="engine precision of the --profile run")
     return ap.parse_args()
 
 
@@ -709,7 +711,7 @@ def profile_arm(args):
     d = lambda a: torch.as_tensor(np.ascontiguousarray(a)).cuda()  # noqa: E731
     ph = d(sc.phase_history)
     geo = [d(v) for v in (sc.ant_x, sc.ant_y, sc.ant_z, sc.slant_range, sc.start_freq)]
-    with focusing.Plan.for_scene(sc, "mixed", device=0) as plan:
+    with focusing.Plan.for_scene(sc, args.profile_precision, device=0) as plan:
         img = plan.new_image("cuda")
         for _ in range(2):
             plan.focus(ph, *geo, out=img)

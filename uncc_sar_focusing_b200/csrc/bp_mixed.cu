@@ -45,6 +45,13 @@ using namespace tile;
 #endif
 constexpr int kFastUnroll = SARBP_FAST_UNROLL;
 
+// CTAs per SM the register budget is sized for when shared memory allows
+// more than one (launch bounds of the default instantiation)
+#ifndef SARBP_CTAS_PER_SM
+#define SARBP_CTAS_PER_SM 2
+#endif
+constexpr int kCtasPerSm = SARBP_CTAS_PER_SM;
+
 
 // One pulse into the thread's MX x 2 pixels.  The two columns l = 0, 1 of a
 // row form a pair and all of their geometry arithmetic runs as paired FP32
@@ -473,8 +480,9 @@ cudaError_t launch_mx_pb(const BpLaunch &L, bool checked, size_t smem, cudaStrea
     // two CTAs per SM (128 registers) by default; one CTA per SM (up to 255
     // registers) when the stage needs more shared memory than two CTAs get
     const bool one_cta = smem > 113u * 1024u;
-    if (checked) return one_cta ? launch_kernels<MX, PB, true, 1>(L, smem, s) : launch_kernels<MX, PB, true, 2>(L, smem, s);
-    return one_cta ? launch_kernels<MX, PB, false, 1>(L, smem, s) : launch_kernels<MX, PB, false, 2>(L, smem, s);
+    if (checked)
+        return one_cta ? launch_kernels<MX, PB, true, 1>(L, smem, s) : launch_kernels<MX, PB, true, kCtasPerSm>(L, smem, s);
+    return one_cta ? launch_kernels<MX, PB, false, 1>(L, smem, s) : launch_kernels<MX, PB, false, kCtasPerSm>(L, smem, s);
 }
 
 template <typename K>
@@ -495,7 +503,7 @@ template <int MX, int PB>
 int resident_mx_pb(size_t smem) {
     const bool one_cta = smem > 113u * 1024u;
     return one_cta ? resident_of(bp_mixed_kernel<MX, PB, false, 1, false>, smem)
-                   : resident_of(bp_mixed_kernel<MX, PB, false, 2, false>, smem);
+                   : resident_of(bp_mixed_kernel<MX, PB, false, kCtasPerSm, false>, smem);
 }
 
 template <int MX, int PB, int MINB>
