@@ -163,7 +163,11 @@ typedef struct sarbp_plan_info {
     long long tiles;
     long long smem_bytes;
     int kernels_per_backproject;
-    int reserved[5];
+    int fused_range_compression; /* 1: one kernel does taper, zero pad, inverse FFT and pair
+                                    rows (mixed precision, nfft = R K, K in {256, 512, 1024},
+                                    R in {1, 2, 4, 8, 16}); 0: taper kernel, cuFFT, pair-row
+                                    kernel */
+    int reserved[4];
 } sarbp_plan_info;
 SARBP_API int sarbp_plan_get_info(const sarbp_plan *plan, sarbp_plan_info *info);
 

@@ -200,3 +200,27 @@ def test_volumetric_config_per_slice(F):
     assert max(per_slice) < MIXED_TOL, per_slice
     got64 = F.focus_scene(sc, "fp64")
     assert O.rel_l2(got64, want) < FP64_TOL
+
+
+@pytest.mark.parametrize("K,R", [(256, 8), (512, 8), (1024, 8), (512, 1), (256, 16), (1024, 2)])
+def test_fused_range_compression_matches_oracle(F, K, R, monkeypatch):
+    """nfft = R K with K in {256, 512, 1024} takes the fused range-compression
+    kernel (taper, zero pad, inverse FFT and pair rows in one launch): its
+    profiles match the FP64 oracle as the cuFFT path's do, and the focused
+    image matches the cuFFT path's."""
+    sc = small_scene(K=K, nfft=R * K, Np=24)
+    want = O.range_compress_fp64(sc.phase_history, sc.nfft, O.hamming(sc.num_range_samples))
+    with F.Plan.for_scene(sc, "mixed") as plan:
+        assert plan.info["fused_range_compression"] == 1
+        plan.range_compress(sc.phase_history)
+        got = plan.range_profiles()
+        img = plan.focus(sc.phase_history, sc.ant_x, sc.ant_y, sc.ant_z, sc.slant_range, sc.start_freq)
+    assert O.rel_l2(got, want) < 2e-6
+    monkeypatch.setenv("SARBP_RC", "cufft")
+    with F.Plan.for_scene(sc, "mixed") as plan:
+        assert plan.info["fused_range_compression"] == 0
+        plan.range_compress(sc.phase_history)
+        got_fft = plan.range_profiles()
+        ref = plan.focus(sc.phase_history, sc.ant_x, sc.ant_y, sc.ant_z, sc.slant_range, sc.start_freq)
+    assert O.rel_l2(got_fft, want) < 2e-6
+    assert O.rel_l2(img, ref) < 2e-6

@@ -59,7 +59,8 @@ class PlanDesc(ctypes.Structure):
 class PlanInfo(ctypes.Structure):
     _fields_ = [("tile_mx", ctypes.c_int), ("stage_pulses", ctypes.c_int), ("window_bins", ctypes.c_int),
                 ("resident_ctas", ctypes.c_int), ("tiles", ctypes.c_longlong), ("smem_bytes", ctypes.c_longlong),
-                ("kernels_per_backproject", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
+                ("kernels_per_backproject", ctypes.c_int), ("fused_range_compression", ctypes.c_int),
+                ("reserved", ctypes.c_int * 4)]
 
 
 class BatchInfo(ctypes.Structure):

@@ -122,6 +122,7 @@ void release(sarbp_plan *p) {
     cudaFree(p->d_gout);
     cudaFree(p->d_hyp);
     cudaFree(p->d_sk);
+    cudaFree(p->d_rctab);
     delete p;
 }
 
@@ -162,6 +163,13 @@ int range_compress_impl(sarbp_plan *p, const void *ph, int np, int memory, cudaS
     if (memory == SARBP_MEMORY_HOST) {
         SARBP_TRY_CUDA(cudaMemcpyAsync(p->d_ph, ph, static_cast<size_t>(np) * p->K * 8, cudaMemcpyHostToDevice, s));
         src = p->d_ph;
+    }
+    if (p->d_rctab) {
+        SARBP_TRY_CUDA(launch_rc_fused(src, p->d_fac, p->d_rctab, p->d_pairs, p->K, p->rc_R, np, p->row_stride,
+                                       p->guard, p->rc_grid, s));
+        p->np_ready = np;
+        if (memory == SARBP_MEMORY_HOST) SARBP_TRY_CUDA(cudaStreamSynchronize(s));
+        return SARBP_OK;
     }
     SARBP_TRY_CUDA(launch_rc_prep(p->precision, src, p->d_fac, p->d_fft, p->K, p->nfft, np, s));
     const cufftResult r0 = cufftSetStream(p->fft, s);
@@ -631,6 +639,34 @@ int sarbp_plan_create(const sarbp_plan_desc *desc, sarbp_plan **out) {
             return from_cuda(e);
         }
     }
+    // fused range compression when the shape has a kernel (environment
+    // SARBP_RC=cufft keeps the taper / cuFFT / pair-row path)
+    {
+        const int K = p->K, N = p->nfft;
+        const int R = (N % K == 0) ? N / K : 0;
+        const char *env = std::getenv("SARBP_RC");
+        const bool want = !(env && std::strcmp(env, "cufft") == 0);
+        size_t rc_smem = 0;
+        std::vector<float> tab;
+        int dev_smem = 0, sms = 0;
+        cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaGetLastError();
+        if (want && p->precision == SARBP_PRECISION_MIXED && R >= 1 && rc_fused_shape(K, R, &rc_smem, &tab) &&
+            rc_smem <= static_cast<size_t>(dev_smem)) {
+            if (alloc(p, &p->d_rctab, tab.size() * sizeof(float)) == SARBP_OK &&
+                cudaMemcpy(p->d_rctab, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess) {
+                p->rc_R = R;
+                // CTAs resident at once: the kernel loops over pulses
+                const int per_sm = rc_smem > 0 ? static_cast<int>((228u * 1024u) / (rc_smem + 1024u)) : 1;
+                p->rc_grid = (sms > 0 ? sms : 148) * (per_sm > 0 ? (per_sm < 4 ? per_sm : 4) : 1);
+            } else {
+                cudaGetLastError();
+                cudaFree(p->d_rctab);
+                p->d_rctab = nullptr;
+            }
+        }
+    }
     const cufftResult r = cufftPlan1d(&p->fft, p->nfft, p->precision == SARBP_PRECISION_FP64 ? CUFFT_Z2Z : CUFFT_C2C,
                                       p->np_cap);
     if (r != CUFFT_SUCCESS) {
@@ -669,6 +705,7 @@ int sarbp_plan_get_info(const sarbp_plan *plan, sarbp_plan_info *info) {
                   g.nz;
     info->smem_bytes = static_cast<long long>(plan->smem);
     info->kernels_per_backproject = (plan->d_sk && plan->sk_resident > 0 && info->tiles % plan->sk_resident != 0) ? 2 : 1;
+    info->fused_range_compression = plan->d_rctab ? 1 : 0;
     return SARBP_OK;
 }
 
@@ -689,6 +726,9 @@ int sarbp_get_range_profiles(sarbp_plan *plan, void *out, int memory, void *stre
     SARBP_TRY(drain_pipe(plan));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t bytes = static_cast<size_t>(plan->np_ready) * plan->nfft * cplx_bytes(plan);
+    if (plan->d_rctab)  // fused range compression keeps the profiles only in the pair rows
+        SARBP_TRY_CUDA(launch_pairs_to_rc(plan->d_pairs, plan->d_fft, plan->nfft, plan->np_ready, plan->row_stride,
+                                          plan->guard, s));
     SARBP_TRY_CUDA(cudaMemcpyAsync(out, plan->d_fft, bytes,
                                    memory == SARBP_MEMORY_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
                                    s));

@@ -15,6 +15,9 @@
 //  3. rc_pairs_kernel stores pair entries {rc[b], rc[b+1] - rc[b]} in rows of
 //     `row_stride` entries with `guard` zero entries on each side, the layout
 //     the backprojection kernels stage into shared memory.
+#include <cmath>
+#include <vector>
+
 #include "sarbp_internal.h"
 
 namespace sarbp {
@@ -116,6 +119,170 @@ __global__ void rc_pairs_batch_kernel(const BatchScene *__restrict__ scenes) {
     }
 }
 
+// ---- fused range compression: nfft = R K, K = 32 K2 ------------------------
+//
+// With y[k] = fac[k] ph[k] (taper x 1/N x shift twiddle) and N = R K the
+// zero-padded inverse DFT splits into R inverse DFTs of length K:
+//     rc[R m + r] = sum_k (y[k] W_N^{k r}) W_K^{k m},   W_L = exp(+j 2 pi / L).
+// One CTA per pulse (grid-stride), one warp per sub-transform r.  Each
+// length-K transform is done in four steps with K = 32 K2, k = k1 + 32 k2,
+// m = m2 + K2 m1:  lane k1 transforms its K2 samples in registers (over k2),
+// multiplies by W_K^{k1 m2}, the warp transposes through shared memory, and
+// lane m2 transforms the 32 values over k1 in registers.  The R results are
+// read back interleaved to write the pair entries {rc[b], rc[b+1] - rc[b]},
+// b = -1 .. N-1, straight to HBM: 8 bytes read per input sample, 16 bytes
+// written per pair entry, no FFT buffer.  Twiddles come from one table built
+// in double on the host and staged into shared memory.
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
+template <int L>
+__host__ __device__ constexpr int log2_of() {
+    int n = 0;
+    for (int v = L; v > 1; v >>= 1) ++n;
+    return n;
+}
+
+template <int L>
+__device__ __forceinline__ constexpr int bit_reverse(int x) {
+    int r = 0;
+    for (int b = 1; b < L; b <<= 1) {
+        r = (r << 1) | (x & 1);
+        x >>= 1;
+    }
+    return r;
+}
+
+// In-register inverse DFT of L points: radix-2 decimation in frequency,
+// natural-order input, bit-reversed output; tw[e] = exp(+j 2 pi e / L).
+template <int L>
+__device__ __forceinline__ void ifft_dif(float2 (&v)[L], const float2 *tw) {
+    constexpr int LOG = log2_of<L>();
+#pragma unroll
+    for (int st = 0; st < LOG; ++st) {
+        const int half = (L >> 1) >> st;
+#pragma unroll
+        for (int i = 0; i < L; i += 2 * half) {
+#pragma unroll
+            for (int j = 0; j < half; ++j) {
+                const float2 a = v[i + j], b = v[i + j + half];
+                v[i + j] = make_float2(a.x + b.x, a.y + b.y);
+                const float2 d = make_float2(a.x - b.x, a.y - b.y);
+                const int e = j * (L / (2 * half));
+                v[i + j + half] = e == 0 ? d : cmulf(d, tw[e]);
+            }
+        }
+    }
+}
+
+// Layout of the twiddle table (complex64 entries) for K = 32 K2, N = R K.
+template <int K2, int R>
+struct RcTable {
+    static constexpr int K = 32 * K2, N = K * R, NW = N / 32;
+    static constexpr int kTwk = 0;                 // W_K^{k1 m2} at m2 * 32 + k1
+    static constexpr int kTw32 = kTwk + K;         // W_32^e, e < 16
+    static constexpr int kTwk2 = kTw32 + 16;       // W_K2^e, e < K2 / 2
+    static constexpr int kWn = kTwk2 + K2 / 2;     // W_N^i, i < 32 R
+    static constexpr int kWnr = kWn + 32 * R;      // W_{N/32}^i, i < N / 32
+    static constexpr int kSize = kWnr + NW;
+    static constexpr int kReg = K + 36;            // shared row of one sub-transform (2 kReg = 8 mod 32)
+    static constexpr size_t kSmem = (static_cast<size_t>(K) + kSize + static_cast<size_t>(R) * kReg) * 8;
+};
+
+template <int K2, int R>
+__global__ void __launch_bounds__(32 * R) rc_fused_kernel(const float2 *__restrict__ ph,
+                                                         const float2 *__restrict__ fac,
+                                                         const float2 *__restrict__ tab, float4 *__restrict__ pairs,
+                                                         int np, long long row_stride, int guard) {
+    using T = RcTable<K2, R>;
+    constexpr int K = T::K, N = T::N, REG = T::kReg, LOGR = log2_of<R>();
+    extern __shared__ __align__(16) float2 rc_sm[];
+    float2 *y = rc_sm, *tb = y + K, *regions = tb + T::kSize;
+    const int tid = threadIdx.x, r = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < T::kSize; i += 32 * R) tb[i] = tab[i];
+    float2 *reg = regions + r * REG;
+    for (int p = blockIdx.x; p < np; p += gridDim.x) {
+        __syncthreads();  // the previous pulse's reads of the regions are done; the table is staged
+        for (int k = tid; k < K; k += 32 * R) y[k] = cmulf(ph[static_cast<long long>(p) * K + k], fac[k]);
+        __syncthreads();
+        // z[k1 + 32 k2] = y[.] W_N^{k1 r} W_{N/32}^{k2 r}, transformed over k2
+        const float2 a = tb[T::kWn + lane * r];
+        float2 v[K2];
+#pragma unroll
+        for (int k2 = 0; k2 < K2; ++k2)
+            v[k2] = cmulf(y[lane + 32 * k2], cmulf(a, tb[T::kWnr + ((k2 * r) & (T::NW - 1))]));
+        ifft_dif<K2>(v, tb + T::kTwk2);
+        // times W_K^{k1 m2}, transposed: element (k1, m2) at m2 * 33 + k1
+#pragma unroll
+        for (int m2 = 0; m2 < K2; ++m2) reg[m2 * 33 + lane] = cmulf(v[bit_reverse<K2>(m2)], tb[T::kTwk + m2 * 32 + lane]);
+        __syncwarp();
+        float2 w[32];
+        if (lane < K2) {
+#pragma unroll
+            for (int k1 = 0; k1 < 32; ++k1) w[k1] = reg[lane * 33 + k1];
+        }
+        __syncwarp();
+        if (lane < K2) {
+            ifft_dif<32>(w, tb + T::kTw32);
+#pragma unroll
+            for (int m1 = 0; m1 < 32; ++m1) reg[lane + K2 * m1] = w[bit_reverse<32>(m1)];
+        }
+        __syncthreads();
+        // rc[R m + r] = regions[r][m]
+        float4 *row = pairs + static_cast<long long>(p) * row_stride + guard;
+        for (int b = tid - 1; b < N; b += 32 * R) {
+            float2 u = make_float2(0.0f, 0.0f), un = make_float2(0.0f, 0.0f);
+            if (b >= 0) u = regions[(b & (R - 1)) * REG + (b >> LOGR)];
+            if (b + 1 < N) un = regions[((b + 1) & (R - 1)) * REG + ((b + 1) >> LOGR)];
+            row[b] = make_float4(u.x, u.y, un.x - u.x, un.y - u.y);
+        }
+    }
+}
+
+template <int K2, int R>
+void fill_rc_table(std::vector<float> &t) {
+    using T = RcTable<K2, R>;
+    t.assign(2 * static_cast<size_t>(T::kSize), 0.0f);
+    auto put = [&](int at, double num, double den) {
+        const double a = 2.0 * M_PI * num / den;
+        t[2 * static_cast<size_t>(at)] = static_cast<float>(std::cos(a));
+        t[2 * static_cast<size_t>(at) + 1] = static_cast<float>(std::sin(a));
+    };
+    for (int m2 = 0; m2 < K2; ++m2)
+        for (int k1 = 0; k1 < 32; ++k1) put(T::kTwk + m2 * 32 + k1, static_cast<double>(k1) * m2, T::K);
+    for (int e = 0; e < 16; ++e) put(T::kTw32 + e, e, 32);
+    for (int e = 0; e < K2 / 2; ++e) put(T::kTwk2 + e, e, K2);
+    for (int i = 0; i < 32 * R; ++i) put(T::kWn + i, i, T::N);
+    for (int i = 0; i < T::NW; ++i) put(T::kWnr + i, i, T::NW);
+}
+
+template <int K2, int R>
+cudaError_t launch_fused(const float2 *ph, const float2 *fac, const float2 *tab, float4 *pairs, int np,
+                         long long row_stride, int guard, int grid, cudaStream_t s) {
+    using T = RcTable<K2, R>;
+    auto kern = rc_fused_kernel<K2, R>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(T::kSmem));
+    if (e != cudaSuccess) return e;
+    const int g = np < grid ? np : grid;
+    kern<<<g > 0 ? g : 1, 32 * R, T::kSmem, s>>>(ph, fac, tab, pairs, np, row_stride, guard);
+    return cudaGetLastError();
+}
+
+// Range profiles rc[b] back out of the pair rows (sarbp_get_range_profiles
+// after fused range compression).
+__global__ void pairs_to_rc_kernel(const float4 *__restrict__ pairs, float2 *__restrict__ rc, int nfft,
+                                   long long total, long long row_stride, int guard) {
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long p = i / nfft;
+        const int b = static_cast<int>(i - p * nfft);
+        const float4 e = pairs[p * row_stride + guard + b];
+        rc[i] = make_float2(e.x, e.y);
+    }
+}
+
 int grid_for(long long total) {
     long long blocks = (total + 255) / 256;
     const long long cap = 148LL * 16;
@@ -159,6 +326,42 @@ cudaError_t launch_rc_prep_batch(const BatchScene *scenes, int nscenes, cudaStre
 cudaError_t launch_rc_pairs_batch(const BatchScene *scenes, int nscenes, cudaStream_t s) {
     if (nscenes < 1 || nscenes > 65535) return cudaErrorInvalidValue;
     rc_pairs_batch_kernel<<<dim3(128, nscenes), 256, 0, s>>>(scenes);
+    return cudaGetLastError();
+}
+
+#define SARBP_RC_SHAPES(X) \
+    X(8, 1) X(8, 2) X(8, 4) X(8, 8) X(8, 16) X(16, 1) X(16, 2) X(16, 4) X(16, 8) X(16, 16) X(32, 1) X(32, 2) \
+        X(32, 4) X(32, 8) X(32, 16)
+
+bool rc_fused_shape(int K, int R, size_t *smem, std::vector<float> *table) {
+#define SARBP_RC_CASE(K2_, R_)                                        \
+    if (K == 32 * K2_ && R == R_) {                                   \
+        if (smem) *smem = RcTable<K2_, R_>::kSmem;                    \
+        if (table) fill_rc_table<K2_, R_>(*table);                    \
+        return true;                                                  \
+    }
+    SARBP_RC_SHAPES(SARBP_RC_CASE)
+#undef SARBP_RC_CASE
+    return false;
+}
+
+cudaError_t launch_rc_fused(const void *ph, const void *fac, const void *table, void *pairs, int K, int R, int np,
+                            long long row_stride, int guard, int grid, cudaStream_t s) {
+#define SARBP_RC_CASE(K2_, R_)                                                                                   \
+    if (K == 32 * K2_ && R == R_)                                                                                 \
+        return launch_fused<K2_, R_>(static_cast<const float2 *>(ph), static_cast<const float2 *>(fac),          \
+                                     static_cast<const float2 *>(table), static_cast<float4 *>(pairs), np,        \
+                                     row_stride, guard, grid, s);
+    SARBP_RC_SHAPES(SARBP_RC_CASE)
+#undef SARBP_RC_CASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_pairs_to_rc(const void *pairs, void *rc, int nfft, int np, long long row_stride, int guard,
+                               cudaStream_t s) {
+    const long long total = static_cast<long long>(np) * nfft;
+    pairs_to_rc_kernel<<<grid_for(total), 256, 0, s>>>(static_cast<const float4 *>(pairs), static_cast<float2 *>(rc),
+                                                      nfft, total, row_stride, guard);
     return cudaGetLastError();
 }
 

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstddef>
+#include <vector>
 #include <cuda_runtime.h>
 #include <cufft.h>
 
@@ -102,6 +103,16 @@ cudaError_t launch_rc_pairs(int precision, const void *fft_buf, void *pairs, int
 // Range compression steps 1 and 3 for every scene of a batch in one launch
 // each (blockIdx.y = scene); the FFT in between runs per scene.
 cudaError_t launch_rc_prep_batch(const BatchScene *scenes, int nscenes, cudaStream_t s);
+// Fused range compression (mixed precision): taper, zero pad, inverse FFT and
+// pair rows in one kernel for nfft = R K with K = 32 K2, K2 in {8, 16, 32},
+// R in {1, 2, 4, 8, 16}.  rc_fused_shape says whether (K, R) is one of those
+// and fills the twiddle table (interleaved float re, im) and the kernel's
+// shared-memory bytes; grid: CTAs (each loops over pulses).
+bool rc_fused_shape(int K, int R, size_t *smem, std::vector<float> *table);
+cudaError_t launch_rc_fused(const void *ph, const void *fac, const void *table, void *pairs, int K, int R, int np,
+                            long long row_stride, int guard, int grid, cudaStream_t s);
+cudaError_t launch_pairs_to_rc(const void *pairs, void *rc, int nfft, int np, long long row_stride, int guard,
+                               cudaStream_t s);
 cudaError_t launch_rc_pairs_batch(const BatchScene *scenes, int nscenes, cudaStream_t s);
 
 }  // namespace sarbp
@@ -130,6 +141,9 @@ struct sarbp_plan {
     double *d_gout;   // adjoint output staging for host outputs [4][np] (allocated on first use)
     void *d_hyp;      // host-memory staging for hypothesis batches (allocated on first use)
     size_t hyp_bytes;
+    void *d_rctab;    // twiddle table of the fused range compression (null: cuFFT path)
+    int rc_R;         // nfft / K of the fused range compression
+    int rc_grid;      // its CTAs
     void *d_sk;       // partial sums of tiles split over CTAs (BpLaunch::sk_partial)
     size_t sk_bytes;
     int sk_resident;  // resident CTAs of the plan's forward kernel
