@@ -635,7 +635,11 @@ def gpu_arm(args):
         bound, roof, tmin = roofline_bound(peaks)
         bp_rate = pp / (bp_ms * 1e-3)
         hbm, hbm_kind = measured_hbm()
-        rc_bytes = sc.num_pulses * (sc.num_range_samples * 8 + sc.nfft * 8)
+        info = plan.info
+        # range compression moves at least the phase history in and the pair
+        # rows the backprojection reads out: 8 B per sample + 16 B per entry
+        # (nfft + 1 entries per pulse)
+        rc_bytes = sc.num_pulses * (sc.num_range_samples * 8 + (sc.nfft + 1) * 16)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -655,11 +659,14 @@ def gpu_arm(args):
                     "api": "sarbp_focus_submit/sarbp_focus_wait, pinned host buffers",
                     "synchronous": {"value": world * pp / e2e_sync_s, "ms_per_step": e2e_sync_s * 1e3,
                                     "api": "sarbp_focus, pinned host buffers"}},
-            # per step: rc_prep, rc_pairs, the backprojection (+ its fix-up
-            # when the tiles are split over the resident CTAs); cuFFT's
-            # kernel is the library's, not counted
-            "gpu_launches": (2 + plan.info["kernels_per_backproject"]) * args.steps,
+            # per step: range compression (one fused kernel, or taper + pair
+            # rows around cuFFT, whose kernel is the library's and not
+            # counted), the backprojection (+ its fix-up when the tiles are
+            # split over the resident CTAs)
+            "gpu_launches": ((1 if info["fused_range_compression"] else 2) + info["kernels_per_backproject"])
+            * args.steps,
             "kernels": {"bp_ms": bp_ms, "range_compress_ms": rc_ms,
+                        "range_compress_fused": bool(info["fused_range_compression"]),
                         "range_compress_hbm": {"bytes": rc_bytes, "achieved_gbs": rc_bytes / (rc_ms * 1e-3) / 1e9,
                                                "peak_gbs": hbm, "peak_kind": hbm_kind,
                                                "frac": rc_bytes / (rc_ms * 1e-3) / 1e9 / hbm}},
