@@ -285,6 +285,19 @@ SARBP_API int sarbp_batch_get_info(const sarbp_batch *batch, sarbp_batch_info *i
 /* Force a schedule: 1 one CTA per tile, 0 split, -1 automatic (default). */
 SARBP_API int sarbp_batch_set_schedule(sarbp_batch *batch, int per_tile);
 
+/* Matched-filter focusing, the reference's other algorithm
+ * (cpuBackProjection.hpp:165-228, matlab/mfBasic.m:73-89):
+ *     img[q] = sum_p sum_k w_k ph_p[k] exp(+j 4 pi (f0_p + k dF) dR_pq / c)
+ * on the plan's grid, with dF = c / (2 max_wr) and the plan's taper w; no
+ * 1/nfft scale, so a well-sampled image is nfft times sarbp_focus's (the
+ * difference is backprojection's interpolation error).  Every pulse is used,
+ * as in MATLAB; the reference's C++ loop skips pulses 0 and 1 (:216-218).
+ * K times the work of backprojection: a reference for it on small images.
+ * Precision as the plan's (MIXED: FP64 phases, FP32 Horner and sums,
+ * complex64 image; FP64: complex128). */
+SARBP_API int sarbp_matched_filter(sarbp_plan *plan, const sarbp_aperture *aperture, void *image, int image_memory,
+                                   void *stream);
+
 /* One call, no plan kept: create, focus, destroy (host or device buffers). */
 SARBP_API int sarbp_focus_image(const sarbp_plan_desc *desc, const sarbp_aperture *aperture, void *image,
                       int image_memory);

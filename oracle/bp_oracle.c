@@ -492,3 +492,48 @@ int oracle_bp_grad_fp64(int Np, int nfft, const double *rc, const double *ax, co
     free(r_vec);
     return 0;
 }
+
+/* ------------------------------------------------------------------------- */
+/* matched filter, FP64                                                       */
+/* ------------------------------------------------------------------------- */
+
+/*
+ * Matched-filter image (matlab/mfBasic.m:73-89; cpuBackProjection.hpp:165-228):
+ *     img[q] += ph_p[k] * exp(+j 4 pi (f0_p + k dF) dR_pq / c)
+ * for pulses p >= first_pulse and samples k < K, dR = |a_p - x_q| - R0_p,
+ * every term in double with cos / sin of the full phase.  ph: complex128
+ * [Np][K] (any taper already applied).  first_pulse = 0 is MATLAB's loop;
+ * the reference C++ loop starts at pulse 2 (cpuBackProjection.hpp:216-218).
+ * img: complex128 [nz][nx][ny].
+ */
+int oracle_mf_fp64(int Np, int K, const double *ph, const double *ax, const double *ay, const double *az,
+                   const double *r0, const double *f0, double df, int nx, int ny, int nz, double x0, double y0,
+                   double z0, double wx, double wy, double wz, int first_pulse, double *img) {
+    if (Np <= 0 || K <= 0 || nx <= 0 || ny <= 0 || nz <= 0 || !ph || !img) return -1;
+    const long long nxy = (long long)nx * ny;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long long row = 0; row < (long long)nz * nx; row++) {
+        const int iz = (int)(row / nx), ix = (int)(row % nx);
+        const double x = grid_coord(ix, nx, x0, wx);
+        const double z = grid_coord(iz, nz, z0, wz);
+        for (int iy = 0; iy < ny; iy++) {
+            const double y = grid_coord(iy, ny, y0, wy);
+            double acc_re = 0.0, acc_im = 0.0;
+            for (int p = first_pulse; p < Np; p++) {
+                const double dx = ax[p] - x, dy = ay[p] - y, dz = az[p] - z;
+                const double dR = sqrt(dx * dx + dy * dy + dz * dz) - r0[p];
+                const double *s = ph + 2 * (size_t)p * K;
+                for (int k = 0; k < K; k++) {
+                    const double phi = 4.0 * ORACLE_PI * (f0[p] + (double)k * df) * dR / ORACLE_CLIGHT;
+                    const double c = cos(phi), sn = sin(phi);
+                    acc_re += s[2 * k] * c - s[2 * k + 1] * sn;
+                    acc_im += s[2 * k] * sn + s[2 * k + 1] * c;
+                }
+            }
+            const long long o = (long long)iz * nxy + (long long)ix * ny + iy;
+            img[2 * o] = acc_re;
+            img[2 * o + 1] = acc_im;
+        }
+    }
+    return 0;
+}

@@ -52,9 +52,11 @@ def lib():
                                       + [_c.c_double] * 4 + [_f64p])
         L.oracle_bp_grad_fp64.argtypes = ([_c.c_int, _c.c_int, _f64p] + bp_geo + [_f64p] * 5)
         L.oracle_dft_c128.argtypes = [_c.c_int, _f64p, _f64p, _c.c_int]
+        L.oracle_mf_fp64.argtypes = ([_c.c_int, _c.c_int, _f64p] + [_f64p] * 5 + [_c.c_double] + [_c.c_int] * 3
+                                     + [_c.c_double] * 6 + [_c.c_int, _f64p])
         for f in ("oracle_range_compress_fp64", "oracle_range_compress_ref32", "oracle_bp_fp64",
                   "oracle_bp_fp64_pixels", "oracle_bp_ref32", "oracle_dft_c128", "oracle_range_compress_ref64",
-                  "oracle_bp_ref64", "oracle_bp_grad_fp64"):
+                  "oracle_bp_ref64", "oracle_bp_grad_fp64", "oracle_mf_fp64"):
             getattr(L, f).restype = _c.c_int
         _LIB = L
     return _LIB
@@ -73,6 +75,9 @@ def ref_lib(fast: bool = False):
                                        + [_c.c_float] * 4 + [_f32p, _f32p, _f32p])
         L.ref_focus_bp_f64.argtypes = ([_c.c_int, _c.c_int] + [_f64p] * 6 + [_c.c_int, _c.c_int]
                                        + [_c.c_double] * 4 + [_f64p, _f64p, _f64p])
+        L.ref_focus_mf_f64.argtypes = ([_c.c_int, _c.c_int] + [_f64p] * 6 + [_c.c_int, _c.c_int]
+                                       + [_c.c_double] * 4 + [_f64p])
+        L.ref_focus_mf_f64.restype = _c.c_int
         L.ref_focus_bp_f32.restype = _c.c_int
         L.ref_focus_bp_f64.restype = _c.c_int
         _REF[key] = L
@@ -246,6 +251,43 @@ def reference_focus(scene, precision: str = "f32", fast: bool = False, pulses: O
     _check(fn(nfft, Np, ph.view(dtype).reshape(-1), freq, *geo, g.nx, g.ny, g.x0, g.y0, g.wx, g.wy,
               img.view(dtype).reshape(-1), max_wy, start_f), "reference focus_SAR_image")
     return img, float(max_wy[0]), start_f
+
+
+def mf_fp64(scene, first_pulse: int = 0) -> np.ndarray:
+    """FP64 matched-filter image of a scenes.Scene ([nz, nx, ny]): taper w
+    applied to the phase history, freq_k = f0_p + k dF, all pulses from
+    first_pulse on (matlab/mfBasic.m:73-89)."""
+    w = window_for(scene.window, scene.num_range_samples)
+    ph = scene.phase_history.astype(np.complex128)
+    if w is not None:
+        ph = ph * w[None, :]
+    ph = np.ascontiguousarray(ph)
+    g = scene.grid
+    out = np.empty((g.nz, g.nx, g.ny), dtype=np.complex128)
+    _check(lib().oracle_mf_fp64(scene.num_pulses, scene.num_range_samples, ph.view(np.float64).reshape(-1),
+                                *_geo(scene.ant_x, scene.ant_y, scene.ant_z, scene.slant_range, scene.start_freq),
+                                float(scene.delta_freq), g.nx, g.ny, g.nz, g.x0, g.y0, g.z0, g.wx, g.wy, g.wz,
+                                int(first_pulse), out.view(np.float64).reshape(-1)), "mf_fp64")
+    return out
+
+
+def reference_mf(scene) -> np.ndarray:
+    """The reference's run_mf<double> (focus_SAR_image with MATCHED_FILTER) on a
+    scene ([nx, ny]); the taper is applied beforehand, as for backprojection."""
+    K = scene.num_range_samples
+    w = window_for(scene.window, K)
+    ph = scene.phase_history.astype(np.complex128)
+    if w is not None:
+        ph = ph * w[None, :]
+    ph = np.ascontiguousarray(ph)
+    freq = scene.start_freq[0] + np.arange(K, dtype=np.float64) * scene.delta_freq
+    geo = [np.ascontiguousarray(v, dtype=np.float64) for v in (scene.ant_x, scene.ant_y, scene.ant_z,
+                                                               scene.slant_range)]
+    g = scene.grid
+    img = np.empty((g.nx, g.ny), dtype=np.complex128)
+    _check(ref_lib().ref_focus_mf_f64(K, scene.num_pulses, ph.view(np.float64).reshape(-1), freq, *geo, g.nx, g.ny,
+                                      g.x0, g.y0, g.wx, g.wy, img.view(np.float64).reshape(-1)), "reference run_mf")
+    return img
 
 
 def rel_l2(a: np.ndarray, b: np.ndarray) -> float:

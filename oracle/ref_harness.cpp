@@ -41,7 +41,7 @@ struct QuietReference {
 template <typename T>
 int focus_with_reference(int nfft, int Np, const T *ph, const T *freq, const T *ax, const T *ay, const T *az,
                          const T *r0, int nx, int ny, T x0, T y0, T wx, T wy, T *img, T *max_wy_out,
-                         T *start_f_out) {
+                         T *start_f_out, bool matched_filter = false) {
     QuietReference quiet;
     SAR_Aperture<T> ap;
     SAR_ImageFormationParameters<T> params;
@@ -69,6 +69,7 @@ int focus_with_reference(int nfft, int Np, const T *ph, const T *freq, const T *
     ap.polarity_channel = 0;
     if (initialize_SAR_Aperture_Data(ap) != EXIT_SUCCESS) return -1;
     params.update(ap);
+    if (matched_filter) params.algorithm = SAR_ImageFormationParameters<T>::ALGORITHM::MATCHED_FILTER;
 
     CArray<T> out(params.N_y_pix * params.N_x_pix);
     focus_SAR_image(ap, params, out);
@@ -92,6 +93,16 @@ int ref_focus_bp_f32(int nfft, int Np, const float *ph, const float *freq, const
                      float *img, float *max_wy_out, float *start_f_out) {
     return focus_with_reference<float>(nfft, Np, ph, freq, ax, ay, az, r0, nx, ny, x0, y0, wx, wy, img,
                                        max_wy_out, start_f_out);
+}
+
+/* run_mf<double> via focus_SAR_image<double,double> with the MATCHED_FILTER
+ * algorithm (cpuBackProjection.hpp:165-228); K = nfft samples per pulse, no
+ * zero pad needed. */
+int ref_focus_mf_f64(int K, int Np, const double *ph, const double *freq, const double *ax, const double *ay,
+                     const double *az, const double *r0, int nx, int ny, double x0, double y0, double wx,
+                     double wy, double *img) {
+    return focus_with_reference<double>(K, Np, ph, freq, ax, ay, az, r0, nx, ny, x0, y0, wx, wy, img, nullptr,
+                                        nullptr, true);
 }
 
 /* run_bp<double> via focus_SAR_image<double,double>. */

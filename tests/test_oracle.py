@@ -149,3 +149,43 @@ def test_fp64_gradient_oracle_matches_central_differences():
             fd = (L(*up) - L(*dn)) / (2 * h)
             want = ga[axis][p] if axis < 3 else gr[p]
             assert abs(fd - want) < 2e-5 * scale, (p, axis, fd, want)
+
+
+# ---- matched filter (cpuBackProjection.hpp:165-228, matlab/mfBasic.m:73-89) ----
+
+def _mf_scene(**kw):
+    from uncc_sar_focusing_b200 import scenes as S
+
+    args = dict(K=32, Np=24, n=16, spacing=0.1, nfft=256, snr_db=None, seed=5, n_targets=2, extent=1.0)
+    args.update(kw)
+    return S.point_target_scene(**args)
+
+
+def test_mf_oracle_matches_direct_sum():
+    from uncc_sar_focusing_b200 import scenes as S
+
+    sc = _mf_scene(K=8, Np=5, n=4, spacing=0.3, nfft=64, n_targets=1, extent=0.5, seed=6)
+    ph = sc.phase_history.astype(complex) * O.window_for(sc.window, 8)
+    img = np.zeros((4, 4), complex)
+    for ix, x in enumerate(sc.grid.axis("x")):
+        for iy, y in enumerate(sc.grid.axis("y")):
+            for p in range(sc.num_pulses):
+                dR = np.sqrt((sc.ant_x[p] - x) ** 2 + (sc.ant_y[p] - y) ** 2 + sc.ant_z[p] ** 2) - sc.slant_range[p]
+                f = sc.start_freq[p] + np.arange(8) * sc.delta_freq
+                img[ix, iy] += np.sum(ph[p] * np.exp(1j * 4 * np.pi * f * dR / S.CLIGHT))
+    assert O.rel_l2(O.mf_fp64(sc)[0], img) < 1e-12
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference not compiled here")
+def test_mf_oracle_pinned_to_reference_run_mf():
+    """The reference's run_mf<double> starts at pulse 2 (cpuBackProjection.hpp:
+    216-218); with the same start the oracle matches it to its float dR."""
+    sc = _mf_scene()
+    ref = O.reference_mf(sc)
+    assert O.rel_l2(O.mf_fp64(sc, first_pulse=2)[0], ref) < 3e-5
+    assert O.rel_l2(O.mf_fp64(sc)[0], ref) > 0.05  # the skipped pulses matter
+
+
+def test_mf_is_nfft_times_bp_up_to_interpolation():
+    sc = _mf_scene(K=64, Np=48, n=32, spacing=0.15, nfft=512, snr_db=20.0, seed=3, n_targets=4, extent=4.0)
+    assert O.rel_l2(O.focus_fp64(sc) * sc.nfft, O.mf_fp64(sc)) < 0.03

@@ -40,7 +40,7 @@ EXPORTED = (
     "sarbp_focus", "sarbp_focus_image", "sarbp_plan_check", "sarbp_backproject_noalloc",
     "sarbp_backproject_adjoint", "sarbp_backproject_hypotheses", "sarbp_focus_submit", "sarbp_focus_wait", "sarbp_plan_get_info",
     "sarbp_batch_create", "sarbp_batch_destroy", "sarbp_batch_focus", "sarbp_batch_wait", "sarbp_batch_autotune",
-    "sarbp_batch_get_info", "sarbp_batch_set_schedule",
+    "sarbp_batch_get_info", "sarbp_batch_set_schedule", "sarbp_matched_filter",
 )
 
 
@@ -116,6 +116,7 @@ def lib():
         L.sarbp_batch_autotune.argtypes = [vp, P(Aperture), P(vp), vp, P(ctypes.c_double)]
         L.sarbp_batch_get_info.argtypes = [vp, P(BatchInfo)]
         L.sarbp_batch_set_schedule.argtypes = [vp, i]
+        L.sarbp_matched_filter.argtypes = [vp, P(Aperture), vp, i, vp]
         for name in EXPORTED:
             if name != "sarbp_status_string":
                 getattr(L, name).restype = i

@@ -123,6 +123,7 @@ void release(sarbp_plan *p) {
     cudaFree(p->d_hyp);
     cudaFree(p->d_sk);
     cudaFree(p->d_rctab);
+    cudaFree(p->d_win);
     delete p;
 }
 
@@ -526,6 +527,64 @@ int focus_wait_impl(sarbp_plan *p, unsigned long long ticket) {
     return st;
 }
 
+int matched_filter_impl(sarbp_plan *p, const sarbp_aperture *ap, void *image, int image_memory, cudaStream_t s) {
+    if (!ap || !image || !ap->phase_history) return SARBP_ERR_NULL_POINTER;
+    const sarbp_geometry *geo = &ap->geometry;
+    if (!geo->ant_x || !geo->ant_y || !geo->ant_z || !geo->slant_range || !geo->start_freq)
+        return SARBP_ERR_NULL_POINTER;
+    const int np = geo->num_pulses;
+    if (np < 1 || np > p->np_cap ||
+        (ap->phase_history_memory != SARBP_MEMORY_HOST && ap->phase_history_memory != SARBP_MEMORY_DEVICE) ||
+        (geo->memory != SARBP_MEMORY_HOST && geo->memory != SARBP_MEMORY_DEVICE) ||
+        (image_memory != SARBP_MEMORY_HOST && image_memory != SARBP_MEMORY_DEVICE))
+        return SARBP_ERR_INVALID_ARGUMENT;
+    if (p->desc.window == SARBP_WINDOW_HAMMING && !p->d_win) {
+        std::vector<double> w(static_cast<size_t>(p->K), 1.0);
+        for (int k = 0; k < p->K && p->K > 1; ++k)
+            w[k] = 0.54 - 0.46 * std::cos(2.0 * M_PI * static_cast<double>(k) / static_cast<double>(p->K - 1));
+        SARBP_TRY(alloc(p, reinterpret_cast<void **>(&p->d_win), w.size() * sizeof(double)));
+        SARBP_TRY_CUDA(cudaMemcpy(p->d_win, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    const void *ph = ap->phase_history;
+    if (ap->phase_history_memory == SARBP_MEMORY_HOST) {
+        SARBP_TRY_CUDA(cudaMemcpyAsync(p->d_ph, ph, static_cast<size_t>(np) * p->K * 8, cudaMemcpyHostToDevice, s));
+        ph = p->d_ph;
+    }
+    const double *gp[5];
+    SARBP_TRY(device_geometry(p, geo, s, gp));
+    const sarbp_grid &g = p->desc.grid;
+    const size_t img_bytes = static_cast<size_t>(g.nx) * g.ny * g.nz * cplx_bytes(p);
+    void *dimg = image_memory == SARBP_MEMORY_HOST ? p->d_img : image;
+    MfLaunch M{};
+    M.ax = gp[0];
+    M.ay = gp[1];
+    M.az = gp[2];
+    M.r0 = gp[3];
+    M.f0 = gp[4];
+    M.np = np;
+    M.K = p->K;
+    M.df = kClight / (2.0 * p->desc.max_wr);
+    M.nx = g.nx;
+    M.ny = g.ny;
+    M.nz = g.nz;
+    M.left = p->left;
+    M.bottom = p->bottom;
+    M.zlow = p->zlow;
+    M.dx = p->dx;
+    M.dy = p->dy;
+    M.dz = p->dz;
+    M.img = dimg;
+    SARBP_TRY_CUDA(launch_mf(ph, p->desc.window == SARBP_WINDOW_HAMMING ? p->d_win : nullptr, M,
+                             p->precision == SARBP_PRECISION_FP64, s));
+    if (image_memory == SARBP_MEMORY_HOST) {
+        SARBP_TRY_CUDA(cudaMemcpyAsync(image, dimg, img_bytes, cudaMemcpyDeviceToHost, s));
+        return read_errors(p, s);
+    }
+    if (geo->memory == SARBP_MEMORY_HOST || ap->phase_history_memory == SARBP_MEMORY_HOST)
+        SARBP_TRY_CUDA(cudaStreamSynchronize(s));
+    return SARBP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -800,6 +859,15 @@ int sarbp_focus_wait(sarbp_plan *plan, unsigned long long ticket) {
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
     return focus_wait_impl(plan, ticket);
+}
+
+int sarbp_matched_filter(sarbp_plan *plan, const sarbp_aperture *aperture, void *image, int image_memory,
+                         void *stream) {
+    if (!plan) return SARBP_ERR_NULL_POINTER;
+    DeviceGuard guard(plan->device);
+    SARBP_TRY_CUDA(guard.status);
+    SARBP_TRY(drain_pipe(plan));
+    return matched_filter_impl(plan, aperture, image, image_memory, static_cast<cudaStream_t>(stream));
 }
 
 int sarbp_plan_check(sarbp_plan *plan, void *stream) {

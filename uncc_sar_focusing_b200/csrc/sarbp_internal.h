@@ -55,6 +55,18 @@ struct BatchScene {
     long long unit_begin, tile_begin;
 };
 
+// Matched-filter launch (mf.cu): geometry on the device, pixel grid, image
+// complex64 (MIXED) or complex128 (FP64) [nz][nx][ny].
+struct MfLaunch {
+    const double *ax, *ay, *az, *r0, *f0;
+    int np, K;
+    double df;  // frequency step (Hz)
+    int nx, ny, nz;
+    double left, bottom, zlow, dx, dy, dz;
+    void *img;
+};
+cudaError_t launch_mf(const void *ph, const double *win, const MfLaunch &M, bool fp64, cudaStream_t s);
+
 // Tile shape of the forward kernels (see bp_mixed.cu).
 struct TileConfig {
     int mx;   // rows per thread; tile = (8*mx) x 64 pixels, 256 threads
@@ -141,6 +153,7 @@ struct sarbp_plan {
     double *d_gout;   // adjoint output staging for host outputs [4][np] (allocated on first use)
     void *d_hyp;      // host-memory staging for hypothesis batches (allocated on first use)
     size_t hyp_bytes;
+    double *d_win;    // taper w_k for the matched filter (allocated on first use)
     void *d_rctab;    // twiddle table of the fused range compression (null: cuFFT path)
     int rc_R;         // nfft / K of the fused range compression
     int rc_grid;      // its CTAs

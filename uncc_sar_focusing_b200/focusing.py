@@ -274,6 +274,23 @@ class Plan:
             inflight.pop(old)
         N.check(st, "sarbp_focus_wait")
 
+    def matched_filter(self, phase_history, ant_x, ant_y, ant_z, slant_range, start_freq, out=None):
+        """Matched-filter image on the plan's grid (sarbp_matched_filter):
+        nfft times the backprojection image up to its interpolation error."""
+        geo, keep = self._geometry(ant_x, ant_y, ant_z, slant_range, start_freq)
+        if int(phase_history.shape[0]) != geo.num_pulses:
+            raise ValueError("phase history and geometry disagree on the pulse count")
+        pp, pmem, pkeep = _ptr(phase_history, np.complex64, geo.num_pulses * self.K)
+        ap = N.Aperture(pp, pmem, geo)
+        if out is None:
+            out = self.new_image(None if pmem == N.MEMORY_HOST and geo.memory == N.MEMORY_HOST else "cuda")
+        ip, imem, ikeep = _ptr(out, self.image_dtype, int(np.prod(self.image_shape())))
+        st = N.lib().sarbp_matched_filter(self._h, ctypes.byref(ap), ip, imem, _stream(out, phase_history, ant_x))
+        N.check(st, "sarbp_matched_filter")
+        if imem == N.MEMORY_HOST and ikeep is not out:
+            np.copyto(out, ikeep.reshape(out.shape))
+        return out
+
     def check(self) -> None:
         """Synchronise and raise if a kernel recorded an error."""
         import torch
