@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     __syncthreads();
 
     const int nblocks = (L.np + PB - 1) / PB;
-    if (nblocks > 0) produce_slots<PB>(L, 0, geo, win_addr, bar_base, warp, lane, cx, cy, cz);
+    if (nblocks > 0) produce_slots<PB>(L, 0, geo, nullptr, win_addr, bar_base, warp, lane, 0, cx, cy, cz);
     __syncthreads();
 
     int last_issued = 0;
@@ -185,8 +185,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     for (int b = 0; b < nblocks; ++b) {
         const int s = b & 1;
         if (b + 1 < nblocks) {
-            produce_slots<PB>(L, b + 1, geo + (s ^ 1) * PB, win_addr + (s ^ 1) * PB * pulse_bytes,
-                              bar_base + 8 * (s ^ 1), warp, lane, cx, cy, cz);
+            produce_slots<PB>(L, b + 1, geo + (s ^ 1) * PB, nullptr, win_addr + (s ^ 1) * PB * pulse_bytes,
+                              bar_base + 8 * (s ^ 1), warp, lane, 0, cx, cy, cz);
             last_issued = b + 1;
         }
         const bool ok = mbar_wait_bounded(bar_base + 8 * s, (b >> 1) & 1, L.err);

@@ -60,22 +60,19 @@ constexpr int kCtasPerSm = SARBP_CTAS_PER_SM;
 // Sign conventions avoid negations: nd2 = -|d|^2, so ne = t^2 - |d|^2 = -e,
 // ng = ne (h + t hr) = -g, and the phase / bin add -kr * ng, -lam * ng.
 template <int MX, bool GATE, bool NEAR, bool CHECKED>
-__device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, uint32_t w_addr, uint32_t zero_addr, int i0,
-                                                 int j0, float lam, const float2 (&nd2)[MX],
-                                                 float (&acc_re)[MX][2], float (&acc_im)[MX][2], int wsize,
-                                                 unsigned *err) {
-    const double2 A_al = *reinterpret_cast<const double2 *>(&g.A);
-    const double2 be_B0 = *reinterpret_cast<const double2 *>(&g.beta);
-    const double2 ga_et = *reinterpret_cast<const double2 *>(&g.gam);
+__device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, const float4 *base, uint32_t w_addr,
+                                                 uint32_t zero_addr, int warp, int lane, float lam,
+                                                 const float2 (&nd2)[MX], float (&acc_re)[MX][2],
+                                                 float (&acc_im)[MX][2], int wsize, unsigned *err) {
     const float4 c0 = *reinterpret_cast<const float4 *>(&g.a8r);  // a8r, b1r, g8, e1
     const float4 c1 = *reinterpret_cast<const float4 *>(&g.tx);   // tx, ty, h, hr
     const float4 c2 = *reinterpret_cast<const float4 *>(&g.kr);   // kr, rc, lo, hi
-    // per-thread phase and bin base in FP64, phase reduced to [-pi, pi]
-    const double pd = fma(static_cast<double>(i0), A_al.y, fma(static_cast<double>(j0), be_B0.x, A_al.x));
-    const float P00 = static_cast<float>(kTwoPi * (pd - rint(pd)));
-    const float B00 =
-        static_cast<float>(fma(static_cast<double>(i0), ga_et.x, fma(static_cast<double>(j0), ga_et.y, be_B0.y)));
-    const float t00 = fmaf(static_cast<float>(i0), c1.x, static_cast<float>(j0) * c1.y);
+    // per-thread phase, bin and projection bases: row part + column part,
+    // each reduced in FP64 by the producer (|phase| <= 2 pi)
+    const float4 rowv = base[32 + warp], colv = base[lane];
+    const float P00 = rowv.x + colv.x;
+    const float B00 = rowv.y + colv.y;
+    const float t00 = rowv.z + colv.z;
     float2 t2 = make_float2(t00, t00 + c1.y);
     float2 Pb = make_float2(P00, P00 + c0.y);
     float2 Bb = make_float2(B00, B00 + c0.w);
@@ -236,7 +233,8 @@ __global__ void __launch_bounds__(kThreads, MINB)
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     float4 *zero = reinterpret_cast<float4 *>(smem + 16);
     PulseGeo *geo = reinterpret_cast<PulseGeo *>(smem + 32);
-    const uint32_t win_addr = smem_addr(smem + 32 + 2 * PB * sizeof(PulseGeo));
+    float4 *bases = reinterpret_cast<float4 *>(smem + 32 + 2 * PB * sizeof(PulseGeo));
+    const uint32_t win_addr = smem_addr(smem + 32 + 2 * PB * (sizeof(PulseGeo) + kBaseEntries * sizeof(float4)));
     const uint32_t zero_addr = smem_addr(zero);
     const uint32_t buf_bytes = static_cast<uint32_t>(PB) * static_cast<uint32_t>(L0.wsize) * 16u;
 
@@ -300,15 +298,17 @@ __global__ void __launch_bounds__(kThreads, MINB)
     }
     __syncthreads();
 
-    // records and windows of the producer cursor's unit into buffer s (lane 0
-    // of each warp works)
+    // records, base tables and windows of the producer cursor's unit into
+    // buffer s
     auto produce = [&](int s) {
-        if (lane != 0) return;
+        // every lane of the warp enters: produce_slots gives lane 0 the record
+        // and the copy and uses the whole warp (shuffles) for the base tables
         const BpLaunch &L = *pc.L;
         const double cx = L.left + static_cast<double>(pc.u.tx * TX + TX / 2) * L.dx;
         const double cy = L.bottom + static_cast<double>(pc.u.ty * kTY + kTY / 2) * L.dy;
         const double cz = L.zlow + static_cast<double>(pc.u.iz) * L.dz;
-        produce_slots<PB>(L, pc.u.b, geo + s * PB, win_addr + s * buf_bytes, bar_base + 8 * s, warp, lane, cx, cy,
+        produce_slots<PB>(L, pc.u.b, geo + s * PB, bases + s * PB * kBaseEntries, win_addr + s * buf_bytes,
+                          bar_base + 8 * s, warp, lane, TX / 2, cx, cy,
                           cz, static_cast<long long>(pc.u.hyp) * L.np);
     };
 
@@ -340,23 +340,25 @@ __global__ void __launch_bounds__(kThreads, MINB)
                 constexpr int kUnroll = kFastUnroll > 0 ? kFastUnroll : PB;
 #pragma unroll kUnroll
                 for (int q = 0; q < PB; ++q)
-                    accumulate_pulse<MX, false, false, CHECKED>(geo[s * PB + q], w0 + q * pulse_bytes, zero_addr,
-                                                                i0, j0, lam, nd2, acc_re, acc_im, wsize, L.err);
+                    accumulate_pulse<MX, false, false, CHECKED>(geo[s * PB + q], bases + (s * PB + q) * kBaseEntries,
+                                                                w0 + q * pulse_bytes, zero_addr, warp, lane, lam,
+                                                                nd2, acc_re, acc_im, wsize, L.err);
             } else {
                 for (int q = 0; q < nq; ++q) {
                     const PulseGeo &g = geo[s * PB + q];
+                    const float4 *bq = bases + (s * PB + q) * kBaseEntries;
                     const int flags = g.flags;
                     if (!(flags & PG_ACTIVE)) continue;
                     const uint32_t w = w0 + q * pulse_bytes;
                     if (flags & PG_NEAR)
-                        accumulate_pulse<MX, true, true, CHECKED>(g, w, zero_addr, i0, j0, lam, nd2, acc_re, acc_im,
-                                                                  wsize, L.err);
+                        accumulate_pulse<MX, true, true, CHECKED>(g, bq, w, zero_addr, warp, lane, lam, nd2, acc_re,
+                                                                  acc_im, wsize, L.err);
                     else if (flags & PG_GATE)
-                        accumulate_pulse<MX, true, false, CHECKED>(g, w, zero_addr, i0, j0, lam, nd2, acc_re,
+                        accumulate_pulse<MX, true, false, CHECKED>(g, bq, w, zero_addr, warp, lane, lam, nd2, acc_re,
                                                                    acc_im, wsize, L.err);
                     else
-                        accumulate_pulse<MX, false, false, CHECKED>(g, w, zero_addr, i0, j0, lam, nd2, acc_re,
-                                                                    acc_im, wsize, L.err);
+                        accumulate_pulse<MX, false, false, CHECKED>(g, bq, w, zero_addr, warp, lane, lam, nd2,
+                                                                    acc_re, acc_im, wsize, L.err);
                 }
             }
         }
@@ -548,7 +550,7 @@ int batch_resident_mx_pb(size_t smem) {
 }  // namespace
 
 size_t bp_mixed_smem_bytes(const TileConfig &tc, int wsize) {
-    return 32 + 2 * static_cast<size_t>(tc.pb) * sizeof(PulseGeo) +
+    return 32 + 2 * static_cast<size_t>(tc.pb) * (sizeof(PulseGeo) + kBaseEntries * sizeof(float4)) +
            2 * static_cast<size_t>(tc.pb) * static_cast<size_t>(wsize) * 16;
 }
 

@@ -156,16 +156,49 @@ __device__ __forceinline__ PulseGeo make_geo(const BpLaunch &L, int p, long long
 // Pulse slots of block b handled by this warp (slot q = warp, warp + 8, ...):
 // lane 0 writes the geometry record and either arrives with the window's byte
 // count and issues its bulk copy, or just arrives (inactive / past the end).
+// Per-(tile, pulse) base tables of the mixed forward kernel: entry lane
+// (0..31) is the column part for j0 = 2 lane - 32 and entry 32 + warp (0..7)
+// the row part for i0 = warp - TX/2 of the thread's phase, bin and
+// projection bases: (2 pi frac(j0 beta), j0 eta, j0 ty, 0) and
+// (2 pi frac(A + i0 alpha), B0 + i0 gam, i0 tx, 0), the phase parts reduced
+// modulo one revolution in FP64.  A thread's base is row + column.
+constexpr int kBaseEntries = 32 + kWarps;
+
+// Records (and base tables when base_s != nullptr) and window copies of
+// stage b into one buffer.  Warp w produces slots w, w + 8, ...: lane 0
+// computes the FP64 record, the warp's lanes fill the base tables from it,
+// then lane 0 issues the window's bulk copy (or a plain arrival), whose
+// release on the stage's mbarrier also publishes the tables (__syncwarp
+// orders the other lanes' stores before it).
 template <int PB>
-__device__ __forceinline__ void produce_slots(const BpLaunch &L, int b, PulseGeo *geo_s, uint32_t win_s,
-                                              uint32_t bar, int warp, int lane, double cx, double cy, double cz,
-                                              long long goff = 0) {
-    if (lane != 0) return;
+__device__ __forceinline__ void produce_slots(const BpLaunch &L, int b, PulseGeo *geo_s, float4 *base_s,
+                                              uint32_t win_s, uint32_t bar, int warp, int lane, int tx_half,
+                                              double cx, double cy, double cz, long long goff = 0) {
     for (int q = warp; q < PB; q += kWarps) {
         const int p = b * PB + q;
-        PulseGeo g;
-        g.flags = 0;
-        if (p < L.np) g = make_geo(L, p, goff, cx, cy, cz);
+        PulseGeo g = {};
+        if (lane == 0 && p < L.np) g = make_geo(L, p, goff, cx, cy, cz);
+        if (base_s) {
+            const unsigned full = 0xffffffffu;
+            const double A = __shfl_sync(full, g.A, 0), alpha = __shfl_sync(full, g.alpha, 0);
+            const double beta = __shfl_sync(full, g.beta, 0), B0 = __shfl_sync(full, g.B0, 0);
+            const double gam = __shfl_sync(full, g.gam, 0), eta = __shfl_sync(full, g.eta, 0);
+            const float tx = __shfl_sync(full, g.tx, 0), ty = __shfl_sync(full, g.ty, 0);
+            float4 *tab = base_s + q * kBaseEntries;
+            const int j0 = 2 * lane - kTY / 2;
+            const double pc = static_cast<double>(j0) * beta;
+            tab[lane] = make_float4(static_cast<float>(kTwoPi * (pc - rint(pc))), static_cast<float>(j0 * eta),
+                                    static_cast<float>(j0) * ty, 0.0f);
+            if (lane < kWarps) {
+                const int i0 = lane - tx_half;
+                const double pr = fma(static_cast<double>(i0), alpha, A);
+                tab[32 + lane] = make_float4(static_cast<float>(kTwoPi * (pr - rint(pr))),
+                                             static_cast<float>(fma(static_cast<double>(i0), gam, B0)),
+                                             static_cast<float>(i0) * tx, 0.0f);
+            }
+            __syncwarp();
+        }
+        if (lane != 0) continue;
         geo_s[q] = g;
         if (g.flags & PG_ACTIVE) {
             const uint32_t bytes = static_cast<uint32_t>(L.wsize) * 16u;
