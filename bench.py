@@ -151,7 +151,7 @@ def cpu_reference_rate(scene, seconds: float, threads: int = 0):
     threads = threads or os.cpu_count() or 1
     npix = scene.grid.npix
 
-    def run(pulse_slices):
+    def run(pulse_slices, keep=None):
         outs = [None] * len(pulse_slices)
 
         def work(i, sl):
@@ -170,7 +170,10 @@ def cpu_reference_rate(scene, seconds: float, threads: int = 0):
             t.start()
         for t in ts:
             t.join()
-        return time.perf_counter() - t0
+        dt = time.perf_counter() - t0
+        if keep is not None:
+            keep.extend(outs)
+        return dt
 
     Np = scene.num_pulses
     # calibrate with two pulses per thread (the reference's aperture
@@ -181,11 +184,15 @@ def cpu_reference_rate(scene, seconds: float, threads: int = 0):
     slices = [slice(i * per_thread * stride, (i + 1) * per_thread * stride, stride) for i in range(threads)]
     slices = [s for s in slices if s.start < Np]
     total_pulses = sum(len(range(*s.indices(Np))) for s in slices)
-    dt = run(slices)
-    return {"value": npix * total_pulses / dt, "unit": UNIT, "cores": len(slices), "kind": kind,
-            "sample": f"{total_pulses} of {Np} pulses onto the full {scene.grid.nx}x{scene.grid.ny} grid, "
-                      f"{len(slices)} threads x {per_thread} pulses, {dt:.1f} s",
-            "seconds": dt}
+    images = []
+    dt = run(slices, images)
+    out = {"value": npix * total_pulses / dt, "unit": UNIT, "cores": len(slices), "kind": kind,
+           "sample": f"{total_pulses} of {Np} pulses onto the full {scene.grid.nx}x{scene.grid.ny} grid, "
+                     f"{len(slices)} threads x {per_thread} pulses, {dt:.1f} s",
+           "seconds": dt}
+    if total_pulses == Np:  # every pulse once: the slices add up to the reference's image
+        out["image"] = sum(images)
+    return out
 
 
 def reference_arm(args):
@@ -488,6 +495,14 @@ def profiled_traffic(config: str):
     return None
 
 
+def peak_phase(a, b) -> float:
+    """Phase of a relative to b (rad) at the magnitude peak of b."""
+    import numpy as np
+
+    i = int(np.argmax(np.abs(b).ravel()))
+    return float(np.angle(a.ravel()[i] * np.conj(b.ravel()[i])))
+
+
 def measured_hbm():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -593,6 +608,8 @@ def gpu_arm(args):
         2, args.steps // 3)
     diff = (img_mixed.to(torch.complex128) - img64).abs().pow(2).sum().sqrt()
     rel = float(diff / img64.abs().pow(2).sum().sqrt())
+    img64_h = img64[0].cpu().numpy()
+    phase_err = peak_phase(img_mixed[0].cpu().numpy(), img64_h)
     del plan64, img64
     torch.cuda.empty_cache()
 
@@ -651,7 +668,7 @@ def gpu_arm(args):
                        "l2": "inputs larger than L2 (range-profile pair buffer "
                              f"{plan.workspace_bytes / 2**20:.0f} MiB plan workspace)",
                        "parallelism": f"{world} image slab(s), one per GPU, no data-path collective"},
-            "accuracy": {"rel_l2_mixed_vs_fp64_gpu": rel, "tolerance": 1e-4},
+            "accuracy": {"rel_l2_mixed_vs_fp64_gpu": rel, "peak_phase_error_rad": phase_err, "tolerance": 1e-4},
             "fp64_gpu": {"bp_value": pp / (fp64_ms * 1e-3), "unit": UNIT,
                          "mixed_speedup": (pp / (bp_ms * 1e-3)) / (pp / (fp64_ms * 1e-3))},
             "e2e": {"value": world * pp / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
@@ -689,6 +706,12 @@ def gpu_arm(args):
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_reference_rate(sc, args.cpu_seconds)
             cb.pop("seconds", None)
+            ref_img = cb.pop("image", None)
+            if ref_img is not None:
+                # the reference's float backprojection against the FP64 path
+                r = np.asarray(ref_img, dtype=np.complex128).reshape(img64_h.shape)
+                cb["accuracy"] = {"rel_l2_vs_fp64_gpu": float(np.linalg.norm(r - img64_h) / np.linalg.norm(img64_h)),
+                                  "peak_phase_error_rad": peak_phase(r, img64_h)}
             line["cpu_baseline"] = cb
     if world > 1:
         dist.barrier()
