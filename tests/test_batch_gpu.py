@@ -148,3 +148,21 @@ def test_batch_argument_errors(F):
         batch.focus([dev_args(sc) for sc in scenes], imgs)
         batch.wait()
     torch.cuda.synchronize()
+
+
+def test_fused_range_compression_scenes_in_a_batch(F):
+    """Scenes whose nfft = R K has a fused range-compression kernel (K = 256,
+    512) take it inside the batch's graph, next to a scene on the cuFFT path."""
+    shapes = [(256, 24, 40, 0.2, 2048, "hamming", 21), (512, 16, 33, 0.25, 4096, None, 22),
+              (64, 20, 17, 0.3, 512, None, 23)]
+    scenes = [make(s) for s in shapes]
+    with F.Batch(scenes) as batch:
+        for _ in range(2):  # capture, then replay
+            imgs = batch.new_images()
+            batch.focus([dev_args(sc) for sc in scenes], imgs)
+            batch.wait()
+        assert batch.info["graph"] == 1
+    for sc, img in zip(scenes, imgs):
+        got = img.cpu().numpy()
+        assert O.rel_l2(got, O.focus_fp64(sc)) < 1e-4
+        assert O.rel_l2(got, single(F, sc)) < 1e-5

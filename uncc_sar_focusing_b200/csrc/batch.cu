@@ -12,6 +12,7 @@
 // cuda_focus_SAR_image focuses one aperture per call, allocating and freeing
 // everything each time (cuda_sar_focusing.hpp:526-723).
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -35,6 +36,10 @@ struct sarbp_batch {
     std::vector<long long> row_stride;
     std::vector<double> lambda, dx, dy, dz, left, bottom, zlow;
     void *fft_work = nullptr;
+    std::vector<void *> rctab;     // per scene: fused range-compression table (null: cuFFT path)
+    std::vector<int> rc_R;         // per scene: nfft / K of the fused path
+    std::vector<void *> rc_tables; // the distinct tables (one per (K, R))
+    int rc_grid = 0;
     // tile shape and the per-scene windows it implies
     TileConfig tile{0, 0};
     size_t smem = 0;
@@ -95,6 +100,7 @@ void release(sarbp_batch *b) {
         if (i < static_cast<int>(b->d_fac.size())) cudaFree(b->d_fac[i]);
     }
     cudaFree(b->fft_work);
+    for (void *t : b->rc_tables) cudaFree(t);
     cudaFree(b->d_table);
     cudaFree(b->d_partial);
     cudaFree(b->d_times);
@@ -208,6 +214,7 @@ int fill_table(sarbp_batch *b, const sarbp_aperture *aps, void *const *images) {
         L.vec_store = ((reinterpret_cast<uintptr_t>(images[i]) & 15u) == 0 && (d.grid.ny % 2) == 0) ? 1 : 0;
         L.err = b->d_err;
         L.nhyp = 1;
+        T.fused = b->rctab[i] ? 1 : 0;
         T.ph = a.phase_history;
         T.fac = b->d_fac[i];
         T.fft = b->d_fft[i];
@@ -238,6 +245,11 @@ int enqueue(sarbp_batch *b, cudaStream_t s) {
     SARBP_TRY_CUDA(cudaGetLastError());
     SARBP_TRY_CUDA(launch_rc_prep_batch(b->d_table, n, s));
     for (int i = 0; i < n; ++i) {
+        if (b->rctab[i]) {
+            SARBP_TRY_CUDA(launch_rc_fused_scene(b->d_table + i, b->rctab[i], b->desc[i].num_range_samples,
+                                                 b->rc_R[i], b->rc_grid, s));
+            continue;
+        }
         const cufftResult r0 = cufftSetStream(b->fft[i], s);
         if (r0 != CUFFT_SUCCESS) return from_cufft(r0);
         const cufftResult r1 = cufftExecC2C(b->fft[i], static_cast<cufftComplex *>(b->d_fft[i]),
@@ -344,8 +356,20 @@ int sarbp_batch_create(const sarbp_plan_desc *descs, int num_scenes, sarbp_batch
     b->row_stride.assign(n, 0);
     b->np_now.assign(n, 0);
     for (auto *v : {&b->lambda, &b->dx, &b->dy, &b->dz, &b->left, &b->bottom, &b->zlow}) v->assign(n, 0.0);
+    b->rctab.assign(n, nullptr);
+    b->rc_R.assign(n, 0);
     int st = SARBP_OK;
     size_t work = 0;
+    // fused range compression where the shape has a kernel (environment
+    // SARBP_RC=cufft keeps the cuFFT path); one table per distinct (K, R)
+    const char *rc_env = std::getenv("SARBP_RC");
+    const bool want_fused = !(rc_env && std::strcmp(rc_env, "cufft") == 0);
+    int dev_smem = 0, sms = 0;
+    cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+    b->rc_grid = 2 * (sms > 0 ? sms : 148);
+    std::vector<std::pair<long long, void *>> tab_of;  // key K * 64 + R
     for (int i = 0; i < n && st == SARBP_OK; ++i) {
         const sarbp_plan_desc &d = descs[i];
         b->lambda[i] = static_cast<double>(d.nfft) / d.max_wr;
@@ -361,11 +385,34 @@ int sarbp_batch_create(const sarbp_plan_desc *descs, int num_scenes, sarbp_batch
         const size_t np = static_cast<size_t>(d.num_pulses);
         const size_t pair_bytes = np * static_cast<size_t>(b->row_stride[i]) * 16;
         const size_t fft_bytes = np * d.nfft * sizeof(float2);
-        if ((st = balloc(b, &b->d_pairs[i], pair_bytes)) || (st = balloc(b, &b->d_fft[i], fft_bytes)) ||
+        const int R = d.nfft % d.num_range_samples == 0 ? d.nfft / d.num_range_samples : 0;
+        size_t rc_smem = 0;
+        std::vector<float> tab;
+        const bool fused = want_fused && R >= 1 && rc_fused_shape(d.num_range_samples, R, &rc_smem, &tab) &&
+                           rc_smem <= static_cast<size_t>(dev_smem);
+        if (fused) {
+            const long long key = static_cast<long long>(d.num_range_samples) * 64 + R;
+            void *t = nullptr;
+            for (const auto &kv : tab_of)
+                if (kv.first == key) t = kv.second;
+            if (!t) {
+                if ((st = balloc(b, &t, tab.size() * sizeof(float)))) break;
+                b->rc_tables.push_back(t);
+                tab_of.emplace_back(key, t);
+                if (cudaMemcpy(t, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+                    cudaGetLastError();
+                    st = SARBP_ERR_CUDA;
+                    break;
+                }
+            }
+            b->rctab[i] = t;
+            b->rc_R[i] = R;
+        }
+        if ((st = balloc(b, &b->d_pairs[i], pair_bytes)) || (!fused && (st = balloc(b, &b->d_fft[i], fft_bytes))) ||
             (st = balloc(b, &b->d_fac[i], static_cast<size_t>(d.num_range_samples) * sizeof(float2))))
             break;
         if (cudaMemset(b->d_pairs[i], 0, pair_bytes) != cudaSuccess ||
-            cudaMemset(b->d_fft[i], 0, fft_bytes) != cudaSuccess) {
+            (!fused && cudaMemset(b->d_fft[i], 0, fft_bytes) != cudaSuccess)) {
             cudaGetLastError();
             st = SARBP_ERR_CUDA;
             break;
@@ -377,6 +424,7 @@ int sarbp_batch_create(const sarbp_plan_desc *descs, int num_scenes, sarbp_batch
             st = SARBP_ERR_CUDA;
             break;
         }
+        if (fused) continue;
         // FFT plans share one work area (their executions are serialised)
         cufftResult r = cufftCreate(&b->fft[i]);
         if (r == CUFFT_SUCCESS) {
@@ -393,6 +441,7 @@ int sarbp_batch_create(const sarbp_plan_desc *descs, int num_scenes, sarbp_batch
     }
     if (st == SARBP_OK && work > 0) st = balloc(b, &b->fft_work, work);
     for (int i = 0; i < n && st == SARBP_OK; ++i) {
+        if (!b->fft_ok[i]) continue;
         const cufftResult r = cufftSetWorkArea(b->fft[i], b->fft_work);
         if (r != CUFFT_SUCCESS) st = from_cufft(r);
     }

@@ -81,6 +81,7 @@ __global__ void rc_pairs_kernel(const C *__restrict__ X, E *__restrict__ pairs, 
 // Batch forms: scene blockIdx.y of the table, grid-stride over its elements.
 __global__ void rc_prep_batch_kernel(const BatchScene *__restrict__ scenes) {
     const BatchScene &S = scenes[blockIdx.y];
+    if (S.fused) return;  // range-compressed by its own fused launch
     const float2 *__restrict__ ph = static_cast<const float2 *>(S.ph);
     const float2 *__restrict__ fac = static_cast<const float2 *>(S.fac);
     float2 *__restrict__ out = static_cast<float2 *>(S.fft);
@@ -103,6 +104,7 @@ __global__ void rc_prep_batch_kernel(const BatchScene *__restrict__ scenes) {
 
 __global__ void rc_pairs_batch_kernel(const BatchScene *__restrict__ scenes) {
     const BatchScene &S = scenes[blockIdx.y];
+    if (S.fused) return;
     const float2 *__restrict__ X = static_cast<const float2 *>(S.fft);
     float4 *__restrict__ pairs = static_cast<float4 *>(const_cast<void *>(S.L.pairs));
     const int nfft = S.L.nfft, guard = S.L.guard;
@@ -191,10 +193,9 @@ struct RcTable {
 };
 
 template <int K2, int R>
-__global__ void __launch_bounds__(32 * R) rc_fused_kernel(const float2 *__restrict__ ph,
-                                                         const float2 *__restrict__ fac,
-                                                         const float2 *__restrict__ tab, float4 *__restrict__ pairs,
-                                                         int np, long long row_stride, int guard) {
+__device__ __forceinline__ void rc_fused_body(const float2 *__restrict__ ph, const float2 *__restrict__ fac,
+                                              const float2 *__restrict__ tab, float4 *__restrict__ pairs, int np,
+                                              long long row_stride, int guard) {
     using T = RcTable<K2, R>;
     constexpr int K = T::K, N = T::N, REG = T::kReg, LOGR = log2_of<R>();
     extern __shared__ __align__(16) float2 rc_sm[];
@@ -238,6 +239,24 @@ __global__ void __launch_bounds__(32 * R) rc_fused_kernel(const float2 *__restri
             row[b] = make_float4(u.x, u.y, un.x - u.x, un.y - u.y);
         }
     }
+}
+
+template <int K2, int R>
+__global__ void __launch_bounds__(32 * R) rc_fused_kernel(const float2 *__restrict__ ph,
+                                                         const float2 *__restrict__ fac,
+                                                         const float2 *__restrict__ tab, float4 *__restrict__ pairs,
+                                                         int np, long long row_stride, int guard) {
+    rc_fused_body<K2, R>(ph, fac, tab, pairs, np, row_stride, guard);
+}
+
+// The same for one scene of a batch: every pointer and size from the scene's
+// slot of the device table, so a captured graph replays with new buffers.
+template <int K2, int R>
+__global__ void __launch_bounds__(32 * R) rc_fused_scene_kernel(const BatchScene *__restrict__ scene,
+                                                               const float2 *__restrict__ tab) {
+    const BatchScene &S = *scene;
+    rc_fused_body<K2, R>(static_cast<const float2 *>(S.ph), static_cast<const float2 *>(S.fac), tab,
+                         static_cast<float4 *>(const_cast<void *>(S.L.pairs)), S.L.np, S.row_stride, S.L.guard);
 }
 
 template <int K2, int R>
@@ -352,6 +371,23 @@ cudaError_t launch_rc_fused(const void *ph, const void *fac, const void *table, 
         return launch_fused<K2_, R_>(static_cast<const float2 *>(ph), static_cast<const float2 *>(fac),          \
                                      static_cast<const float2 *>(table), static_cast<float4 *>(pairs), np,        \
                                      row_stride, guard, grid, s);
+    SARBP_RC_SHAPES(SARBP_RC_CASE)
+#undef SARBP_RC_CASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_rc_fused_scene(const BatchScene *scene, const void *table, int K, int R, int grid,
+                                  cudaStream_t s) {
+#define SARBP_RC_CASE(K2_, R_)                                                                                   \
+    if (K == 32 * K2_ && R == R_) {                                                                               \
+        auto kern = rc_fused_scene_kernel<K2_, R_>;                                                               \
+        const size_t smem = RcTable<K2_, R_>::kSmem;                                                              \
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,                   \
+                                             static_cast<int>(smem));                                             \
+        if (e != cudaSuccess) return e;                                                                           \
+        kern<<<grid > 0 ? grid : 1, 32 * R_, smem, s>>>(scene, static_cast<const float2 *>(table));               \
+        return cudaGetLastError();                                                                                \
+    }
     SARBP_RC_SHAPES(SARBP_RC_CASE)
 #undef SARBP_RC_CASE
     return cudaErrorInvalidValue;

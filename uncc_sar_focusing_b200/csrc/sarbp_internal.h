@@ -50,7 +50,7 @@ struct BatchScene {
     const void *fac;            // per-sample taper x scale x shift twiddle [K]
     void *fft;                  // complex64 [np][nfft] FFT buffer
     int K;
-    int pad0;
+    int fused;                  // 1: range-compressed by its own fused launch (batched taper/pair kernels skip it)
     long long row_stride;       // pair entries per pulse row
     long long unit_begin, tile_begin;
 };
@@ -125,6 +125,10 @@ cudaError_t launch_rc_fused(const void *ph, const void *fac, const void *table, 
                             long long row_stride, int guard, int grid, cudaStream_t s);
 cudaError_t launch_pairs_to_rc(const void *pairs, void *rc, int nfft, int np, long long row_stride, int guard,
                                cudaStream_t s);
+// Fused range compression of one batch scene, parameters read from its table
+// slot (grid CTAs loop over the scene's pulses).
+cudaError_t launch_rc_fused_scene(const BatchScene *scene, const void *table, int K, int R, int grid,
+                                  cudaStream_t s);
 cudaError_t launch_rc_pairs_batch(const BatchScene *scenes, int nscenes, cudaStream_t s);
 
 }  // namespace sarbp
