@@ -56,6 +56,14 @@ def test_adjoint_odd_grid_and_swath_edges(torch_cuda):
     assert ea < GRAD_TOL and er < GRAD_TOL, (ea, er)
 
 
+def test_adjoint_partial_last_stage(torch_cuda):
+    # 37 pulses: the last pulse stage of every tile is partly empty
+    sc = S.point_target_scene(K=64, Np=37, n=40, spacing=0.2, nfft=256, snr_db=None, seed=9, n_targets=3,
+                              extent=5.0)
+    ea, er = grads_vs_oracle(torch_cuda, sc, seed=3)
+    assert ea < GRAD_TOL and er < GRAD_TOL, (ea, er)
+
+
 def test_adjoint_near_field(torch_cuda):
     sc = S.point_target_scene(K=64, Np=32, n=64, spacing=0.1, nfft=512, snr_db=None, seed=7, n_targets=3,
                               radius=60.0)

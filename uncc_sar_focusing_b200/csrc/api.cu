@@ -360,8 +360,9 @@ int adjoint_impl(sarbp_plan *p, const sarbp_geometry *geo, const void *grad, int
         SARBP_TRY_CUDA(cudaMemcpyAsync(p->d_img, grad, npix * 8, cudaMemcpyHostToDevice, s));
         dgrad = p->d_img;
     }
-    // stage depth: the deepest of 4, 2, 1 pulses whose shared memory fits
-    TileConfig tc{p->tile.mx, 4};
+    // stage depth: the deepest of 8, 4, 2, 1 pulses whose shared memory fits
+    // two CTAs per SM
+    TileConfig tc{p->tile.mx, 8};
     size_t smem = bp_adjoint_smem_bytes(tc, p->wsize);
     while (tc.pb > 1 && smem > 110u * 1024u) {
         tc.pb /= 2;

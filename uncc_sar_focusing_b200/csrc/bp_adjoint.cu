@@ -11,14 +11,32 @@
 // v'_p(b) is the slope of the linear interpolation, rc[b+1] - rc[b], which the
 // pair entries already hold.  Nothing per pixel-pulse is stored: the kernel
 // recomputes the geometry of every (tile, pulse) exactly as the forward kernel
-// does (same records, same shared-memory windows, same FP32 per-pixel
-// arithmetic).  Per tile and pulse each thread accumulates
-//     E0 = sum s,  Et = sum s t_eff,  Ex = sum s dx_eff,  Ey = sum s dy_eff
-// over its pixels, where Rc/R_q = 1 + t_eff/Rc and d/R_q = d_eff/Rc (far field:
-// t_eff = u.d, d_eff = d; near field: the exact ratios), so that
-//     sum_q s u_q = u (E0 + Et/Rc) - (Ex, Ey, 0)/Rc.
-// The CTA reduces the four sums per pulse and writes the tile's gradient;
-// adjoint_reduce_kernel sums the tiles in double.
+// does (same records, base tables, shared-memory windows and FP32 per-pixel
+// arithmetic).
+//
+// Per pixel the kernel holds G_q as |G_q| exp(j psi_q), so that with
+// nu = kr / lambda and Z = v' + j nu v
+//     s_pq = lambda |G_q| Re(Z exp(j (phi - psi_q))):
+// the conjugate product with G becomes a phase offset folded into the sine /
+// cosine argument, and lambda leaves the pixel loop.  Writing d = (i dx, j dy, 0)
+// for a pixel's offset from the tile centre (i, j its row and column offsets)
+// and Rc/R_q = 1 + t_eff/Rc, d/R_q = d_eff/Rc (far field: t_eff = u.d =
+// i ux dx + j uy dy, d_eff = d; near field: the exact ratios),
+//     sum_q s u_q = u (E0 + Et/Rc) - (dx Ei, dy Ej, 0)/Rc
+// with E0 = sum s, Ei = sum s i (Rc/R), Ej = sum s j (Rc/R) and Et = sum s t_eff.
+// In the far field t_eff is linear in (i, j), so a thread accumulates only
+// sum |G| Re(..) per column and sum row * |G| Re(..) over its pixels (two
+// paired FP32 accumulators) and Et follows from Ei and Ej.
+//
+// Work split: the (tile, pulse-stage) units are divided over the resident
+// CTAs in contiguous ranges (bp_tile.cuh); every unit writes the per-tile
+// partial gradients of its own pulses, so no fix-up pass is needed.  Stages
+// are up to 8 pulses deep (record production and the stage barrier are paid
+// per stage); the warp reduces the 4 sums of each group of up to 4 pulses with
+// one transposed butterfly (each step halves the values a lane holds), the
+// CTA adds its 8 warps, and
+// adjoint_reduce_kernel sums the tiles per pulse in double, in a fixed order.
+#include <algorithm>
 #include <cstdint>
 
 #include "bp_common.cuh"
@@ -30,21 +48,23 @@ namespace {
 
 using namespace tile;
 
-template <int MX, bool NEAR>
-__device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, uint32_t w_addr, uint32_t zero_addr, int i0, int j0,
-                                              float lam, const float2 (&nd2)[MX], const float2 (&G)[MX][2],
-                                              const float (&dxk)[MX], const float (&dyl)[2], float4 &E) {
-    const double2 A_al = *reinterpret_cast<const double2 *>(&g.A);
-    const double2 be_B0 = *reinterpret_cast<const double2 *>(&g.beta);
-    const double2 ga_et = *reinterpret_cast<const double2 *>(&g.gam);
+// Far field: T += |G| s~ per column (x: l = 0, y: l = 1; s~ = Re(Z exp(j
+// theta))) and, after each of the thread's rows k = 0..MX-2, V += T, so that
+// sum_k k |G| s~ = (MX - 1) T - V without per-row weights.
+// Near field: E += (s^, s^ r i, s^ r j, s^ Rc (r - 1)), s^ = |G| s~, r = Rc/R.
+template <int MX, bool GATE, bool NEAR>
+__device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, const float4 *base, uint32_t w_addr,
+                                              uint32_t zero_addr, int warp, int lane, float lam,
+                                              const float2 (&nd2)[MX], const float2 (&npsi)[MX],
+                                              const float2 (&gm)[MX], float i0f, float j0f, float inv_lam, float2 &T,
+                                              float2 &V, float4 &E) {
     const float4 c0 = *reinterpret_cast<const float4 *>(&g.a8r);  // a8r, b1r, g8, e1
     const float4 c1 = *reinterpret_cast<const float4 *>(&g.tx);   // tx, ty, h, hr
     const float4 c2 = *reinterpret_cast<const float4 *>(&g.kr);   // kr, rc, lo, hi
-    const double pd = fma(static_cast<double>(i0), A_al.y, fma(static_cast<double>(j0), be_B0.x, A_al.x));
-    const float P00 = static_cast<float>(kTwoPi * (pd - rint(pd)));
-    const float B00 =
-        static_cast<float>(fma(static_cast<double>(i0), ga_et.x, fma(static_cast<double>(j0), ga_et.y, be_B0.y)));
-    const float t00 = fmaf(static_cast<float>(i0), c1.x, static_cast<float>(j0) * c1.y);
+    const float4 rowv = base[32 + warp], colv = base[lane];
+    const float P00 = rowv.x + colv.x;
+    const float B00 = rowv.y + colv.y;
+    const float t00 = rowv.z + colv.z;
     float2 t2 = make_float2(t00, t00 + c1.y);
     float2 Pb = make_float2(P00, P00 + c0.y);
     float2 Bb = make_float2(B00, B00 + c0.w);
@@ -52,7 +72,7 @@ __device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, uint32_t w_addr
     const float2 HR = splat(c1.w), H = splat(c1.z), NKR = splat(-c2.x), NLAM = splat(-lam);
     const float2 MAGIC = splat(kRoundMagic), NMAGIC = splat(-kRoundMagic), NEG1 = splat(-1.0f);
     const uint32_t w_adj = w_addr - kRoundMagicBits * 16u;
-    const float kr = c2.x;
+    const float nu = c2.x * inv_lam;
 #pragma unroll
     for (int k = 0; k < MX; ++k) {
         if (k > 0) {
@@ -72,102 +92,156 @@ __device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, uint32_t w_addr
             const float2 ne = __ffma2_rn(t2, t2, nd2[k]);
             ng = __fmul2_rn(ne, __ffma2_rn(t2, HR, H));
         }
-        const float2 P = __ffma2_rn(NKR, ng, Pb);
+        // theta = phi - psi, bin B and its floor split as in the forward kernel
+        const float2 TH = __ffma2_rn(NKR, ng, __fadd2_rn(Pb, npsi[k]));
         const float2 B = __ffma2_rn(NLAM, ng, Bb);
         const float2 y = __fadd2_rd(B, MAGIC);
         const float2 a = __ffma2_rn(__fadd2_rn(y, NMAGIC), NEG1, B);
+        float2 st;  // s~ of the pair
 #pragma unroll
         for (int l = 0; l < 2; ++l) {
-            const float Pl = l ? P.y : P.x;
-            const float Bl = l ? B.y : B.x;
+            const float Tl = l ? TH.y : TH.x;
             const float yl = l ? y.y : y.x;
             const float al = l ? a.y : a.x;
             float sn, cs;
-            __sincosf(Pl, &sn, &cs);
+            __sincosf(Tl, &sn, &cs);
             uint32_t addr = __float_as_uint(yl) * 16u + w_adj;
-            const bool valid = (Bl > c2.z) && (Bl < c2.w);
-            addr = valid ? addr : zero_addr;
+            if (GATE) {
+                const float Bl = l ? B.y : B.x;
+                const bool valid = (Bl > c2.z) && (Bl < c2.w);
+                addr = valid ? addr : zero_addr;
+            }
             const float4 v = lds128(addr);
             const float vr = fmaf(al, v.z, v.x);
             const float vi = fmaf(al, v.w, v.y);
-            const float2 Gq = G[k][l];
-            // W = conj(G) exp(j phi)
-            const float Wre = fmaf(Gq.x, cs, Gq.y * sn);
-            const float Wim = fmaf(Gq.x, sn, -Gq.y * cs);
-            // s = lambda Re(W v') - kr Im(W v)
-            const float X = fmaf(Wre, v.z, -Wim * v.w);
-            const float Y = fmaf(Wre, vi, Wim * vr);
-            const float s = fmaf(lam, X, -kr * Y);
-            const float tl = l ? t2.y : t2.x;
-            if (NEAR) {
-                const float rl = l ? rr.y : rr.x;
-                // t_eff = Rc (Rc/R - 1), d_eff = d Rc/R
+            // Z = v' + j nu v; s~ = Re(Z exp(j theta))
+            const float zr = fmaf(-nu, vi, v.z);
+            const float zi = fmaf(nu, vr, v.w);
+            const float sl = fmaf(zr, cs, -zi * sn);
+            if (l) st.y = sl;
+            else st.x = sl;
+        }
+        if (NEAR) {
+            const float2 sh = __fmul2_rn(gm[k], st);
+            const float ik = i0f + static_cast<float>(8 * k);
+#pragma unroll
+            for (int l = 0; l < 2; ++l) {
+                const float s = l ? sh.y : sh.x;
+                const float r = l ? rr.y : rr.x;
+                const float sr = s * r;
                 E.x += s;
-                E.y = fmaf(s, c2.y * (rl - 1.0f), E.y);
-                E.z = fmaf(s * rl, dxk[k], E.z);
-                E.w = fmaf(s * rl, dyl[l], E.w);
-            } else {
-                E.x += s;
-                E.y = fmaf(s, tl, E.y);
-                E.z = fmaf(s, dxk[k], E.z);
-                E.w = fmaf(s, dyl[l], E.w);
+                E.y = fmaf(sr, ik, E.y);
+                E.z = fmaf(sr, j0f + static_cast<float>(l), E.z);
+                E.w = fmaf(s, c2.y * (r - 1.0f), E.w);
             }
+        } else {
+            T = __ffma2_rn(gm[k], st, T);
+            if (k < MX - 1) V = __fadd2_rn(V, T);
         }
     }
 }
 
-__device__ __forceinline__ float warp_sum(float v) {
+// The warp sums of N values (N = 4, 8, 16 or 32) at once: each step swaps
+// half of a lane's values with the partner lane and adds, so N - 1 + 5 -
+// log2(N) shuffles give lane L the sum of value (L >> (5 - log2 N)).
+template <int N>
+__device__ __forceinline__ float warp_reduce_scatter(float (&v)[N], int lane) {
+    static_assert(N == 4 || N == 8 || N == 16 || N == 32, "value count");
+    int o = 16;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
+    for (int h = N / 2; h >= 1; h >>= 1, o >>= 1) {
+        const bool upper = (lane & o) != 0;
+#pragma unroll
+        for (int i = 0; i < h; ++i) {
+            const float send = upper ? v[i] : v[i + h];
+            const float keep = upper ? v[i + h] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    float r = v[0];
+#pragma unroll
+    for (; o >= 1; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    return r;
 }
+
+template <int N>
+struct Log2 {
+    static constexpr int value = N <= 1 ? 0 : 1 + Log2<N / 2>::value;
+};
+template <>
+struct Log2<1> {
+    static constexpr int value = 0;
+};
 
 template <int MX, int PB>
 __global__ void __launch_bounds__(kThreads, 2)
-    bp_adjoint_kernel(const BpLaunch L, const float2 *__restrict__ grad, float4 *__restrict__ partials) {
+    bp_adjoint_kernel(const __grid_constant__ BpLaunch L, const float2 *__restrict__ grad,
+                      float4 *__restrict__ partials) {
     constexpr int TX = 8 * MX;
+    constexpr int RG = PB < 4 ? PB : 4;  // pulses per warp reduction
+    constexpr int NV = 4 * RG;           // its sums: (E0, Ei, Ej, Et) per pulse
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     float4 *zero = reinterpret_cast<float4 *>(smem + 16);
     PulseGeo *geo = reinterpret_cast<PulseGeo *>(smem + 32);
-    float4 *red = reinterpret_cast<float4 *>(smem + 32 + 2 * PB * sizeof(PulseGeo));  // [kWarps][PB]
-    const uint32_t win_addr = smem_addr(smem + 32 + 2 * PB * sizeof(PulseGeo) + kWarps * PB * sizeof(float4));
+    float4 *bases = reinterpret_cast<float4 *>(smem + 32 + 2 * PB * sizeof(PulseGeo));
+    float *red = reinterpret_cast<float *>(smem + 32 + 2 * PB * (sizeof(PulseGeo) + kBaseEntries * sizeof(float4)));
+    const uint32_t win_addr = smem_addr(smem + 32 + 2 * PB * (sizeof(PulseGeo) + kBaseEntries * sizeof(float4)) +
+                                        2 * kWarps * 4 * PB * sizeof(float));
     const uint32_t zero_addr = smem_addr(zero);
     const int wsize = L.wsize;
     const uint32_t pulse_bytes = static_cast<uint32_t>(wsize) * 16u;
+    const uint32_t buf_bytes = static_cast<uint32_t>(PB) * pulse_bytes;
+
+    const TileGrid tg = tile_grid(L, TX, PB);
+    const long long G = gridDim.x;
+    const long long lo = sk_lo(blockIdx.x, tg.units, G);
+    const int n = static_cast<int>(sk_lo(blockIdx.x + 1, tg.units, G) - lo);
+    if (n <= 0) return;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int ty0 = blockIdx.x * kTY, tx0 = blockIdx.y * TX, iz = blockIdx.z;
-    const long long tile = (static_cast<long long>(blockIdx.z) * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-    const double cx = L.left + static_cast<double>(tx0 + TX / 2) * L.dx;
-    const double cy = L.bottom + static_cast<double>(ty0 + kTY / 2) * L.dy;
-    const double cz = L.zlow + static_cast<double>(iz) * L.dz;
     const int i0 = warp - TX / 2;
     const int j0 = 2 * lane - kTY / 2;
-    const float lam = static_cast<float>(L.lambda);
+    const float i0f = static_cast<float>(i0), j0f = static_cast<float>(j0);
+    const float lam = static_cast<float>(L.lambda), inv_lam = static_cast<float>(1.0 / L.lambda);
+    const float dxf = static_cast<float>(L.dx), dyf = static_cast<float>(L.dy);
 
-    float2 nd2[MX], G[MX][2];
-    float dxk[MX], dyl[2];
-    {
-        const float dxf = static_cast<float>(L.dx), dyf = static_cast<float>(L.dy);
+    float2 nd2[MX];  // -|d|^2 of the thread's pixel pairs
 #pragma unroll
-        for (int l = 0; l < 2; ++l) dyl[l] = static_cast<float>(j0 + l) * dyf;
+    for (int k = 0; k < MX; ++k) {
+        const float di = static_cast<float>(i0 + 8 * k) * dxf;
+        const float dj0 = j0f * dyf, dj1 = static_cast<float>(j0 + 1) * dyf;
+        nd2[k] = make_float2(-fmaf(di, di, dj0 * dj0), -fmaf(di, di, dj1 * dj1));
+    }
+
+    UnitCursor cc, pc;  // consumer at unit i, producer at unit i + 1
+    cc.init(tg, L, lo);
+    pc = cc;
+
+    // the consumer tile's upstream gradient as -psi and |G| per pixel pair
+    float2 npsi[MX], gm[MX];
+    auto load_tile = [&]() {
+        const int tx0 = cc.tx * TX, ty0 = cc.ty * kTY;
 #pragma unroll
         for (int k = 0; k < MX; ++k) {
-            dxk[k] = static_cast<float>(i0 + 8 * k) * dxf;
-            nd2[k] = make_float2(-fmaf(dxk[k], dxk[k], dyl[0] * dyl[0]), -fmaf(dxk[k], dxk[k], dyl[1] * dyl[1]));
             const int row = tx0 + warp + 8 * k;
+            float ps[2], mg[2];
 #pragma unroll
             for (int l = 0; l < 2; ++l) {
                 const int col = ty0 + 2 * lane + l;
-                G[k][l] = (row < L.nx && col < L.ny)
-                              ? grad[(static_cast<long long>(iz) * L.nx + row) * L.ny + col]
-                              : make_float2(0.0f, 0.0f);
+                const float2 q = (row < L.nx && col < L.ny)
+                                     ? grad[(static_cast<long long>(cc.iz) * L.nx + row) * L.ny + col]
+                                     : make_float2(0.0f, 0.0f);
+                ps[l] = -atan2f(q.y, q.x);
+                mg[l] = sqrtf(fmaf(q.x, q.x, q.y * q.y));
             }
+            npsi[k] = make_float2(ps[0], ps[1]);
+            gm[k] = make_float2(mg[0], mg[1]);
         }
-    }
+    };
+    load_tile();
 
-    const uint32_t bar_base = smem_addr(&bars[0]);
+    const uint32_t bar_base = smem_addr(&bars[0]);  // buffer s barrier at bar_base + 8*s
     if (threadIdx.x == 0) {
         mbar_init(bar_base, PB);
         mbar_init(bar_base + 8, PB);
@@ -176,110 +250,213 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
     __syncthreads();
 
-    const int nblocks = (L.np + PB - 1) / PB;
-    if (nblocks > 0) produce_slots<PB>(L, 0, geo, nullptr, win_addr, bar_base, warp, lane, 0, cx, cy, cz);
+    // records, base tables and windows of the producer cursor's unit into
+    // buffer s (every lane of the warp enters produce_slots)
+    auto produce = [&](int s) {
+        const double cx = L.left + static_cast<double>(pc.tx * TX + TX / 2) * L.dx;
+        const double cy = L.bottom + static_cast<double>(pc.ty * kTY + kTY / 2) * L.dy;
+        const double cz = L.zlow + static_cast<double>(pc.iz) * L.dz;
+        produce_slots<PB>(L, pc.b, geo + s * PB, bases + s * PB * kBaseEntries, win_addr + s * buf_bytes,
+                          bar_base + 8 * s, warp, lane, TX / 2, cx, cy, cz);
+    };
+    produce(0);
     __syncthreads();
 
     int last_issued = 0;
-    bool timed_out = false;
-    for (int b = 0; b < nblocks; ++b) {
-        const int s = b & 1;
-        if (b + 1 < nblocks) {
-            produce_slots<PB>(L, b + 1, geo + (s ^ 1) * PB, nullptr, win_addr + (s ^ 1) * PB * pulse_bytes,
-                              bar_base + 8 * (s ^ 1), warp, lane, 0, cx, cy, cz);
-            last_issued = b + 1;
+    for (int i = 0; i < n; ++i) {
+        const int s = i & 1;
+        if (i + 1 < n) {
+            pc.advance(tg, L);
+            produce(s ^ 1);
+            last_issued = i + 1;
         }
-        const bool ok = mbar_wait_bounded(bar_base + 8 * s, (b >> 1) & 1, L.err);
+        const int b = cc.b;
+        const bool ok = mbar_wait_bounded(bar_base + 8 * s, (i >> 1) & 1, L.err);
         const int nq = min(PB, L.np - b * PB);
-        float4 E[PB];
-#pragma unroll
-        for (int q = 0; q < PB; ++q) {
-            E[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (!ok || q >= nq) continue;
-            const PulseGeo &g = geo[s * PB + q];
-            const int flags = g.flags;
-            if (!(flags & PG_ACTIVE)) continue;
-            const uint32_t w = win_addr + (s * PB + q) * pulse_bytes;
-            if (flags & PG_NEAR)
-                adjoint_pulse<MX, true>(g, w, zero_addr, i0, j0, lam, nd2, G, dxk, dyl, E[q]);
-            else
-                adjoint_pulse<MX, false>(g, w, zero_addr, i0, j0, lam, nd2, G, dxk, dyl, E[q]);
+        // the record fields the final sum of pulse q = threadIdx.x needs
+        int rflags = 0;
+        float rtx = 0.0f, rty = 0.0f, rux = 0.0f, ruy = 0.0f, ruz = 0.0f, rinv = 0.0f;
+        bool fast = false;
+        if (ok) {
+            const int my_flags = lane < nq ? geo[s * PB + lane].flags : 0;
+            const int any_f = __reduce_or_sync(0xffffffffu, my_flags);
+            const int all_f = __reduce_and_sync(0xffffffffu, lane < nq ? my_flags : PG_ACTIVE);
+            fast = nq == PB && (all_f & PG_ACTIVE) && !(any_f & (PG_GATE | PG_NEAR));
+            if (threadIdx.x < nq) {
+                const PulseGeo &g = geo[s * PB + threadIdx.x];
+                rflags = g.flags;
+                rtx = g.tx;
+                rty = g.ty;
+                rux = g.ux;
+                ruy = g.uy;
+                ruz = g.uz;
+                rinv = g.rinv;
+            }
         }
-        // CTA sums per pulse: warp butterflies, then across the 8 warps
+        // pulses in groups of RG: the group's 4 RG sums, then their warp sums
+        // (lane L holds value L >> shift) into this stage's half of red; after
+        // the stage barrier thread q adds the 8 warps for pulse q (the next
+        // stage writes the other half, so one barrier per stage)
+        constexpr int shift = 5 - Log2<NV>::value;
+        float *red_s = red + s * (kWarps * 4 * PB);
+        const uint32_t w0 = win_addr + s * buf_bytes;
 #pragma unroll
-        for (int q = 0; q < PB; ++q) {
-            const float4 r = make_float4(warp_sum(E[q].x), warp_sum(E[q].y), warp_sum(E[q].z), warp_sum(E[q].w));
-            if (lane == 0) red[warp * PB + q] = r;
+        for (int gi = 0; gi < PB / RG; ++gi) {
+            float v[NV];
+#pragma unroll
+            for (int c = 0; c < NV; ++c) v[c] = 0.0f;
+            // far field: E0, Ei = i0 E0 + 8 sum k s^, Ej = j0 E0 + sum_(l=1) s^, Et later
+            auto far_sums = [&](int r, float2 T, float2 V) {
+                const float S = T.x + T.y;
+                const float Sk = fmaf(static_cast<float>(MX - 1), S, -(V.x + V.y));
+                v[4 * r + 0] = S;
+                v[4 * r + 1] = fmaf(i0f, S, 8.0f * Sk);
+                v[4 * r + 2] = fmaf(j0f, S, T.y);
+            };
+            if (fast) {
+#pragma unroll
+                for (int r = 0; r < RG; ++r) {
+                    const int q = gi * RG + r;
+                    float2 T = make_float2(0.0f, 0.0f), V = make_float2(0.0f, 0.0f);
+                    float4 E;
+                    adjoint_pulse<MX, false, false>(geo[s * PB + q], bases + (s * PB + q) * kBaseEntries,
+                                                    w0 + q * pulse_bytes, zero_addr, warp, lane, lam, nd2, npsi, gm,
+                                                    i0f, j0f, inv_lam, T, V, E);
+                    far_sums(r, T, V);
+                }
+            } else if (ok) {
+#pragma unroll
+                for (int r = 0; r < RG; ++r) {
+                    const int q = gi * RG + r;
+                    const PulseGeo &g = geo[s * PB + q];
+                    if (q >= nq || !(g.flags & PG_ACTIVE)) continue;
+                    const float4 *bq = bases + (s * PB + q) * kBaseEntries;
+                    const uint32_t w = w0 + q * pulse_bytes;
+                    float2 T = make_float2(0.0f, 0.0f), V = make_float2(0.0f, 0.0f);
+                    float4 E = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    if (g.flags & PG_NEAR) {
+                        adjoint_pulse<MX, true, true>(g, bq, w, zero_addr, warp, lane, lam, nd2, npsi, gm, i0f, j0f,
+                                                      inv_lam, T, V, E);
+                        v[4 * r + 0] = E.x;
+                        v[4 * r + 1] = E.y;
+                        v[4 * r + 2] = E.z;
+                        v[4 * r + 3] = E.w;
+                    } else {
+                        adjoint_pulse<MX, true, false>(g, bq, w, zero_addr, warp, lane, lam, nd2, npsi, gm, i0f,
+                                                       j0f, inv_lam, T, V, E);
+                        far_sums(r, T, V);
+                    }
+                }
+            }
+            const float rs = warp_reduce_scatter<NV>(v, lane);
+            if ((lane & ((1 << shift) - 1)) == 0) red_s[warp * 4 * PB + gi * NV + (lane >> shift)] = rs;
         }
-        __syncthreads();
-        if (ok && threadIdx.x < nq) {
+        if (__syncthreads_or(!ok)) {
+            // let the copies already issued for the other buffer land before
+            // the CTA's shared memory goes away (again bounded)
+            if (threadIdx.x == 0 && last_issued > i)
+                mbar_wait_bounded(bar_base + 8 * (last_issued & 1), (last_issued >> 1) & 1, L.err);
+            return;
+        }
+        if (threadIdx.x < nq) {
             const int q = threadIdx.x;
-            const int p = b * PB + q;
             float4 t = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
             for (int w = 0; w < kWarps; ++w) {
-                const float4 r = red[w * PB + q];
-                t.x += r.x;
-                t.y += r.y;
-                t.z += r.z;
-                t.w += r.w;
+                const float4 x = *reinterpret_cast<const float4 *>(red_s + w * 4 * PB + 4 * q);
+                t.x += x.x;
+                t.y += x.y;
+                t.z += x.z;
+                t.w += x.w;
             }
-            const PulseGeo &g = geo[s * PB + q];
             float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (g.flags & PG_ACTIVE) {
-                // sum s u_q = u (E0 + Et/Rc) - (Ex, Ey, 0)/Rc; dL/dR0 = -E0
-                const float c = fmaf(t.y, g.rinv, t.x);
-                out.x = fmaf(g.ux, c, -t.z * g.rinv);
-                out.y = fmaf(g.uy, c, -t.w * g.rinv);
-                out.z = g.uz * c;
-                out.w = -t.x;
+            if (rflags & PG_ACTIVE) {
+                // sum s u_q = u (E0 + Et/Rc) - (dx Ei, dy Ej, 0)/Rc, times lambda;
+                // dL/dR0 = -lambda E0
+                const float Et = (rflags & PG_NEAR) ? t.w : fmaf(rtx, t.y, rty * t.z);
+                const float c = fmaf(Et, rinv, t.x);
+                out.x = lam * fmaf(rux, c, -dxf * t.y * rinv);
+                out.y = lam * fmaf(ruy, c, -dyf * t.z * rinv);
+                out.z = lam * ruz * c;
+                out.w = -lam * t.x;
             }
-            partials[tile * L.np + p] = out;
+            const long long tile =
+                ((static_cast<long long>(cc.hyp) * L.nz + cc.iz) * tg.tiles_x + cc.tx) * tg.tiles_y + cc.ty;
+            partials[tile * L.np + b * PB + q] = out;
         }
-        if (__syncthreads_or(!ok)) {
-            timed_out = true;
-            break;
+        if (i + 1 < n) {
+            cc.advance(tg, L);
+            if (cc.b == 0) load_tile();
         }
     }
-    if (timed_out && threadIdx.x == 0 && last_issued > 0)
-        mbar_wait_bounded(bar_base + 8 * (last_issued & 1), (last_issued >> 1) & 1, L.err);
 }
 
-// out[p] = sum over tiles of partials[t][p], in double; layout of the
-// outputs: grad_ant [3][np] (x, y, z) and grad_r0 [np] (may be null).
-__global__ void adjoint_reduce_kernel(const float4 *__restrict__ partials, long long ntiles, int np,
-                                      double *__restrict__ grad_ant, double *__restrict__ grad_r0, int accumulate) {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) {
-        double gx = 0.0, gy = 0.0, gz = 0.0, gr = 0.0;
-        for (long long t = 0; t < ntiles; ++t) {
+// out[p] = sum over tiles of partials[t][p], in double.  Block: 32 pulses
+// (the lanes) x kRedWarps warps; warp w sums tiles w, w + kRedWarps, ...,
+// then warp 0 adds the warps in order (a fixed order: the result does not
+// depend on scheduling).  Outputs: grad_ant [3][np] (x, y, z) and
+// grad_r0 [np] (may be null).
+constexpr int kRedWarps = 16;
+
+__global__ void __launch_bounds__(32 * kRedWarps)
+    adjoint_reduce_kernel(const float4 *__restrict__ partials, long long ntiles, int np, double *__restrict__ grad_ant,
+                          double *__restrict__ grad_r0, int accumulate) {
+    __shared__ double sums[kRedWarps][4][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int p = blockIdx.x * 32 + lane;
+    double gx = 0.0, gy = 0.0, gz = 0.0, gr = 0.0;
+    if (p < np) {
+        for (long long t = w; t < ntiles; t += kRedWarps) {
             const float4 v = partials[t * np + p];
             gx += v.x;
             gy += v.y;
             gz += v.z;
             gr += v.w;
         }
-        if (accumulate) {
-            grad_ant[p] += gx;
-            grad_ant[np + p] += gy;
-            grad_ant[2 * np + p] += gz;
-            if (grad_r0) grad_r0[p] += gr;
-        } else {
-            grad_ant[p] = gx;
-            grad_ant[np + p] = gy;
-            grad_ant[2 * np + p] = gz;
-            if (grad_r0) grad_r0[p] = gr;
-        }
+    }
+    sums[w][0][lane] = gx;
+    sums[w][1][lane] = gy;
+    sums[w][2][lane] = gz;
+    sums[w][3][lane] = gr;
+    __syncthreads();
+    if (w != 0 || p >= np) return;
+    for (int u = 1; u < kRedWarps; ++u) {
+        gx += sums[u][0][lane];
+        gy += sums[u][1][lane];
+        gz += sums[u][2][lane];
+        gr += sums[u][3][lane];
+    }
+    if (accumulate) {
+        grad_ant[p] += gx;
+        grad_ant[np + p] += gy;
+        grad_ant[2 * np + p] += gz;
+        if (grad_r0) grad_r0[p] += gr;
+    } else {
+        grad_ant[p] = gx;
+        grad_ant[np + p] = gy;
+        grad_ant[2 * np + p] = gz;
+        if (grad_r0) grad_r0[p] = gr;
     }
 }
 
 template <int MX, int PB>
 cudaError_t launch_adj(const BpLaunch &L, const void *grad, void *partials, size_t smem, cudaStream_t s) {
     constexpr int TX = 8 * MX;
-    const dim3 grid((L.ny + kTY - 1) / kTY, (L.nx + TX - 1) / TX, L.nz);
     auto kern = bp_adjoint_kernel<MX, PB>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    kern<<<grid, kThreads, smem, s>>>(L, static_cast<const float2 *>(grad), static_cast<float4 *>(partials));
+    // one CTA per resident slot, each taking a contiguous range of units
+    int dev = 0, sms = 0, occ = 0;
+    e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+    const long long units = tile_grid(L, TX, PB).units;
+    const long long ctas = std::min<long long>(units, static_cast<long long>(sms) * occ);
+    if (ctas < 1 || ctas > 0x7fffffffLL) return cudaErrorInvalidValue;
+    kern<<<static_cast<unsigned>(ctas), kThreads, smem, s>>>(L, static_cast<const float2 *>(grad),
+                                                              static_cast<float4 *>(partials));
     return cudaGetLastError();
 }
 
@@ -291,14 +468,18 @@ long long bp_tile_count(const BpLaunch &L, const TileConfig &tc) {
 }
 
 size_t bp_adjoint_smem_bytes(const TileConfig &tc, int wsize) {
-    return 32 + 2 * static_cast<size_t>(tc.pb) * sizeof(PulseGeo) + kWarps * static_cast<size_t>(tc.pb) * 16 +
-           2 * static_cast<size_t>(tc.pb) * static_cast<size_t>(wsize) * 16;
+    const size_t pb = static_cast<size_t>(tc.pb);
+    return 32 + 2 * pb * (sizeof(PulseGeo) + kBaseEntries * sizeof(float4)) + 2 * kWarps * 4 * pb * sizeof(float) +
+           2 * pb * static_cast<size_t>(wsize) * 16;
 }
 
 cudaError_t launch_bp_adjoint(const BpLaunch &L, const void *grad, void *partials, const TileConfig &tc, size_t smem,
                               cudaStream_t s) {
 #define SARBP_ADJ_CASE(MX_, PB_) \
     if (tc.mx == MX_ && tc.pb == PB_) return launch_adj<MX_, PB_>(L, grad, partials, smem, s);
+    SARBP_ADJ_CASE(4, 8)
+    SARBP_ADJ_CASE(2, 8)
+    SARBP_ADJ_CASE(1, 8)
     SARBP_ADJ_CASE(4, 4)
     SARBP_ADJ_CASE(4, 2)
     SARBP_ADJ_CASE(4, 1)
@@ -314,9 +495,9 @@ cudaError_t launch_bp_adjoint(const BpLaunch &L, const void *grad, void *partial
 
 cudaError_t launch_adjoint_reduce(const void *partials, long long ntiles, int np, double *grad_ant, double *grad_r0,
                                   int accumulate, cudaStream_t s) {
-    const int blocks = (np + 255) / 256;
-    adjoint_reduce_kernel<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(static_cast<const float4 *>(partials), ntiles, np,
-                                                                  grad_ant, grad_r0, accumulate);
+    const int blocks = (np + 31) / 32;
+    adjoint_reduce_kernel<<<blocks > 0 ? blocks : 1, 32 * kRedWarps, 0, s>>>(
+        static_cast<const float4 *>(partials), ntiles, np, grad_ant, grad_r0, accumulate);
     return cudaGetLastError();
 }
 
