@@ -60,6 +60,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-autofocus", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU kernels (oracle/_ref/libref_gpu.so)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-configuration section")
     ap.add_argument("--no-volumetric", action="store_true", help="skip the volumetric-configuration section")
     ap.add_argument("--grid-seconds", type=float, default=20.0, help="bound on the grid-search baseline")
@@ -195,6 +197,34 @@ def cpu_reference_rate(scene, seconds: float, threads: int = 0):
     return out
 
 
+def reference_gpu_rate(scene, img64=None, reps: int = 3):
+    """The reference's own GPU kernels on this GPU (oracle/_ref/libref_gpu.so:
+    cuifft + cufftNormalize_1DBatch + cufftShift_1DBatch + backprojection_loop
+    <float>, launched as cuda_focus_SAR_image launches them), CUDA-event
+    timed; with img64 (the FP64 image) also its accuracy."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    if not O.ref_gpu_available():
+        return {"unavailable": "oracle/_ref/libref_gpu.so not built (needs the reference sources at build time)"}
+    try:
+        img, fft_ms, bp_ms = O.reference_gpu_focus(scene, reps=reps)
+    except ValueError as e:
+        return {"unavailable": str(e)}
+    pp = scene.pixel_pulses
+    out = {"value": pp / (bp_ms * 1e-3), "unit": UNIT, "bp_ms": bp_ms, "range_compress_ms": fft_ms,
+           "fft_plus_bp_value": pp / ((bp_ms + fft_ms) * 1e-3),
+           "kind": "reference GPU kernels (cuda_BackProjectionKernels.cuh) built for sm_100a, launched as "
+                   "cuda_focus_SAR_image does; per-call allocation, plan creation and cudaDeviceReset left out",
+           "reps": reps}
+    if img64 is not None:
+        r = img.astype(np.complex128).reshape(img64.shape)
+        out["accuracy"] = {"rel_l2_vs_fp64_gpu": float(np.linalg.norm(r - img64) / np.linalg.norm(img64)),
+                           "peak_phase_error_rad": peak_phase(r, img64)}
+    return out
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -215,6 +245,8 @@ def reference_arm(args):
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
                              "sample": info["sample"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_reference_gpu:
+        line["reference_gpu"] = reference_gpu_rate(sc)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -589,6 +621,13 @@ def gpu_arm(args):
     plan.focus(ph_d, *geo_d, out=img_d)
     bp_ms = max_over_ranks(timed(lambda: plan.backproject(*geo_d, out=img_d), reps)) / reps
     plan.check()
+    # the adjoint (dL/d antenna position and R0) on the same range profiles,
+    # with the image itself as the upstream gradient
+    grad_img = img_d.clone()
+    plan.backproject_adjoint(*geo_d, grad_img)
+    adj_ms = max_over_ranks(timed(lambda: plan.backproject_adjoint(*geo_d, grad_img), reps)) / reps
+    plan.check()
+    del grad_img
     # a second of back-to-back steps so the clock record covers steady load
     t_end = time.perf_counter() + 1.0
     while time.perf_counter() < t_end:
@@ -683,6 +722,10 @@ def gpu_arm(args):
             "gpu_launches": ((1 if info["fused_range_compression"] else 2) + info["kernels_per_backproject"])
             * args.steps,
             "kernels": {"bp_ms": bp_ms, "range_compress_ms": rc_ms,
+                        "adjoint": {"ms": adj_ms, "value": pp / (adj_ms * 1e-3), "unit": UNIT,
+                                    "vs_forward_bp_time": adj_ms / bp_ms,
+                                    "what": "sarbp_backproject_adjoint: adjoint kernel + tile sum, "
+                                            "dL/d(antenna xyz, R0) for all pulses"},
                         "range_compress_fused": bool(info["fused_range_compression"]),
                         "range_compress_hbm": {"bytes": rc_bytes, "achieved_gbs": rc_bytes / (rc_ms * 1e-3) / 1e9,
                                                "peak_gbs": hbm, "peak_kind": hbm_kind,
@@ -713,6 +756,11 @@ def gpu_arm(args):
                 cb["accuracy"] = {"rel_l2_vs_fp64_gpu": float(np.linalg.norm(r - img64_h) / np.linalg.norm(img64_h)),
                                   "peak_phase_error_rad": peak_phase(r, img64_h)}
             line["cpu_baseline"] = cb
+        if world == 1 and not args.no_reference_gpu:
+            rg = reference_gpu_rate(sc, img64_h)
+            if "value" in rg:
+                rg["bp_speedup_of_mixed"] = bp_rate / rg["value"]
+            line["reference_gpu"] = rg
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

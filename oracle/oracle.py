@@ -253,6 +253,44 @@ def reference_focus(scene, precision: str = "f32", fast: bool = False, pulses: O
     return img, float(max_wy[0]), start_f
 
 
+def ref_gpu_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_gpu.so"))
+
+
+def reference_gpu_focus(scene, reps: int = 3):
+    """The reference's own GPU kernels (cuifft, cufftNormalize_1DBatch,
+    cufftShift_1DBatch, backprojection_loop<float>; oracle/ref_gpu_harness.cu)
+    on a scene, timed with CUDA events.  Float geometry as SAR_Aperture<float>
+    holds it; the phase history tapered and zero-padded to Nfft (the reference
+    has neither).  Returns (image [nx, ny] complex64, fft_ms, bp_ms); raises
+    ValueError, before any GPU work, for a scene that reaches the swath's
+    lower edge (the reference kernel would read index -1 there)."""
+    if "gpu" not in _REF:
+        L = ctypes.CDLL(os.path.join(HERE, "_ref", "libref_gpu.so"))
+        L.ref_gpu_focus.argtypes = ([_f32p, _c.c_int, _c.c_int] + [_f32p] * 5 + [_c.c_double, _c.c_int, _c.c_int]
+                                    + [_c.c_double] * 4 + [_c.c_int, _f32p, _c.POINTER(_c.c_double),
+                                                           _c.POINTER(_c.c_double)])
+        L.ref_gpu_focus.restype = _c.c_int
+        _REF["gpu"] = L
+    if scene.grid.nz != 1 or scene.grid.z0 != 0.0:
+        raise ValueError("the reference kernel images the z = 0 plane only")
+    ph, _ = pad_for_reference(scene, np.float32)
+    ph = np.ascontiguousarray(ph)
+    Np, nfft = ph.shape
+    geo = [np.ascontiguousarray(v, dtype=np.float32) for v in (scene.ant_x, scene.ant_y, scene.ant_z,
+                                                               scene.slant_range, scene.start_freq)]
+    g = scene.grid
+    img = np.empty((g.nx, g.ny), dtype=np.complex64)
+    fft_ms, bp_ms = _c.c_double(0.0), _c.c_double(0.0)
+    rc = _REF["gpu"].ref_gpu_focus(ph.view(np.float32).reshape(-1), nfft, Np, *geo, float(scene.max_wr), g.nx, g.ny,
+                                   g.x0, g.y0, g.wx, g.wy, int(reps), img.view(np.float32).reshape(-1),
+                                   _c.byref(fft_ms), _c.byref(bp_ms))
+    if rc == -2:
+        raise ValueError("scene reaches the swath's lower edge: the reference kernel would read index -1")
+    _check(rc, "reference GPU focus")
+    return img, fft_ms.value, bp_ms.value
+
+
 def mf_fp64(scene, first_pulse: int = 0) -> np.ndarray:
     """FP64 matched-filter image of a scenes.Scene ([nz, nx, ny]): taper w
     applied to the phase history, freq_k = f0_p + k dF, all pulses from
