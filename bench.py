@@ -25,7 +25,12 @@ Printed on rank 0 as one JSON line:
   cpu_baseline  the reference's own CPU backprojection (run_bp, compiled from
             its sources into oracle/_ref) on a bounded pulse sample, all host
             threads, rank 0 at N = 1
---impl reference prints the reference CPU implementation's line alone.
+  reference_gpu  the reference's own GPU kernels (oracle/_ref/libref_gpu.so,
+            built from cuda_BackProjectionKernels.cuh) on the same GPU and
+            inputs, CUDA-event timed, with their accuracy against FP64
+  kernels.adjoint  sarbp_backproject_adjoint on the same range profiles
+--impl reference prints the reference CPU implementation's line alone (with
+the reference GPU kernels' timing beside it).
 """
 from __future__ import annotations
 
@@ -66,7 +71,8 @@ def parse_args():
     ap.add_argument("--no-volumetric", action="store_true", help="skip the volumetric-configuration section")
     ap.add_argument("--grid-seconds", type=float, default=20.0, help="bound on the grid-search baseline")
     ap.add_argument("--profile", action="store_true",
-                    help="one warm-up and one focus step of the workload, nothing else (for ncu captures)")
+                    help="one warm-up and one focus step of the workload, then two adjoint calls (mixed), "
+                         "nothing else (for ncu captures)")
     ap.add_argument("--pulses", type=int, default=0, help="use only the first N pulses (profiling)")
     ap.add_argument("--profile-precision", choices=["mixed", "fp64"], default="mixed",
                     help="engine precision of the --profile run")
@@ -770,9 +776,10 @@ def gpu_arm(args):
 
 
 def profile_arm(args):
-    """A single focus of the workload after one warm-up, with the scene
-    synthesis temporaries released first so that a profiler's per-pass memory
-    save/restore only covers the plan and the inputs."""
+    """A single focus of the workload after one warm-up, then (mixed
+    precision) two adjoint calls with the image as the upstream gradient, with
+    the scene synthesis temporaries released first so that a profiler's
+    per-pass memory save/restore only covers the plan and the inputs."""
     import numpy as np
     import torch
 
@@ -793,6 +800,9 @@ def profile_arm(args):
         img = plan.new_image("cuda")
         for _ in range(2):
             plan.focus(ph, *geo, out=img)
+        if args.profile_precision == "mixed":
+            for _ in range(2):
+                plan.backproject_adjoint(*geo, img)
         torch.cuda.synchronize()
         plan.check()
     print(json.dumps({"profile": args.config, "pulses": sc.num_pulses, "pixel_pulses": sc.pixel_pulses}))
