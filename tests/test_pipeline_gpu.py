@@ -121,7 +121,7 @@ def test_plan_info_reports_the_split(F):
     sc = scene(21)
     with F.Plan.for_scene(sc, "mixed") as plan:
         info = plan.info
-        assert info["tile_mx"] in (1, 2, 4) and info["stage_pulses"] >= 1
+        assert info["tile_mx"] in (1, 2, 4, 8) and info["stage_pulses"] >= 1
         assert info["resident_ctas"] > 0 and info["window_bins"] >= 4
         split = info["tiles"] % info["resident_ctas"] != 0
         assert info["kernels_per_backproject"] == (2 if split else 1)

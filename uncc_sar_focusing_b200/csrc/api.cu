@@ -33,10 +33,16 @@ void window_for(const sarbp_plan *p, int mx, int *W, int *wsize) {
 int choose_tile(sarbp_plan *p) {
     // (mx, pb) candidates, best first; the first pass keeps two CTAs per SM
     // for the mixed kernel, the second accepts one CTA per SM (coarse grids
-    // whose range-bin windows are wide)
-    static const int cand[][2] = {{4, 8}, {4, 4}, {2, 8}, {2, 4}, {1, 8}, {1, 4}, {2, 2}, {1, 2}, {1, 1}};
+    // whose range-bin windows are wide).  64-row tiles (mx = 8, mixed only)
+    // halve the per-pulse record, base-table and setup work per pixel: on
+    // 1024 x 2048 x 1024^2 a pixel-pulse costs ~1.87 (mx 8) against ~2.25
+    // (mx 4) time units, so they are taken unless padding the rows to 64
+    // instead of 32 adds more than 15% pixels.
+    static const int cand[][2] = {{8, 8}, {8, 4}, {4, 8}, {4, 4}, {2, 8}, {2, 4}, {1, 8}, {1, 4}, {2, 2}, {1, 2}, {1, 1}};
     const int ncand = static_cast<int>(sizeof(cand) / sizeof(cand[0]));
     const bool fp64 = p->precision == SARBP_PRECISION_FP64;
+    const long long nx = p->desc.grid.nx;
+    const bool tall_tiles = !fp64 && (nx + 63) / 64 * 64 * 100 <= (nx + 31) / 32 * 32 * 115;
     int forced_mx = 0, forced_pb = 0;
     if (const char *env = std::getenv("SARBP_TILE")) {
         if (std::sscanf(env, "%d,%d", &forced_mx, &forced_pb) != 2) forced_mx = forced_pb = 0;
@@ -50,6 +56,7 @@ int choose_tile(sarbp_plan *p) {
                 mx = forced_mx;
                 pb = forced_pb;
             }
+            if (pass >= 0 && mx == 8 && !tall_tiles) continue;
             int W, wsize;
             window_for(p, mx, &W, &wsize);
             if (wsize > (1 << 16)) continue;

@@ -477,6 +477,8 @@ cudaError_t launch_bp_adjoint(const BpLaunch &L, const void *grad, void *partial
                               cudaStream_t s) {
 #define SARBP_ADJ_CASE(MX_, PB_) \
     if (tc.mx == MX_ && tc.pb == PB_) return launch_adj<MX_, PB_>(L, grad, partials, smem, s);
+    SARBP_ADJ_CASE(8, 8)
+    SARBP_ADJ_CASE(8, 4)
     SARBP_ADJ_CASE(4, 8)
     SARBP_ADJ_CASE(2, 8)
     SARBP_ADJ_CASE(1, 8)

@@ -557,6 +557,8 @@ size_t bp_mixed_smem_bytes(const TileConfig &tc, int wsize) {
 int bp_mixed_resident(const TileConfig &tc, size_t smem) {
 #define SARBP_MIXED_CASE(MX_, PB_) \
     if (tc.mx == MX_ && tc.pb == PB_) return resident_mx_pb<MX_, PB_>(smem);
+    SARBP_MIXED_CASE(8, 8)
+    SARBP_MIXED_CASE(8, 4)
     SARBP_MIXED_CASE(4, 16)
     SARBP_MIXED_CASE(4, 8)
     SARBP_MIXED_CASE(4, 4)
@@ -615,6 +617,8 @@ int bp_mixed_batch_resident(const TileConfig &tc, size_t smem) {
 cudaError_t launch_bp_mixed(const BpLaunch &L, const TileConfig &tc, bool checked, size_t smem, cudaStream_t s) {
 #define SARBP_MIXED_CASE(MX_, PB_) \
     if (tc.mx == MX_ && tc.pb == PB_) return launch_mx_pb<MX_, PB_>(L, checked, smem, s);
+    SARBP_MIXED_CASE(8, 8)
+    SARBP_MIXED_CASE(8, 4)
     SARBP_MIXED_CASE(4, 16)
     SARBP_MIXED_CASE(4, 8)
     SARBP_MIXED_CASE(4, 4)
