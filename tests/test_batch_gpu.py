@@ -147,7 +147,8 @@ def test_autotune_keeps_results(F):
         best = batch.autotune(args, imgs)
         assert best > 0.0
         info = batch.info
-        assert (info["tile_mx"], info["stage_pulses"]) in [(4, 8), (4, 4), (2, 8), (2, 4), (1, 8), (1, 4)]
+        assert (info["tile_mx"], info["stage_pulses"]) in [(8, 8), (8, 4), (4, 8), (4, 4), (2, 8), (2, 4), (1, 8),
+                                                           (1, 4)]
         imgs = batch.new_images()
         batch.focus(args, imgs)
         batch.wait()

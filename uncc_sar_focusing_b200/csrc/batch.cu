@@ -152,9 +152,20 @@ bool configure(sarbp_batch *b, const TileConfig &tc) {
 }
 
 int choose_default_tile(sarbp_batch *b) {
+    // 64-row tiles unless padding every scene's rows to 64 instead of 32 adds
+    // more than 15% pixel-pulses over the batch (the plan's rule, api.cu)
+    double pad64 = 0.0, pad32 = 0.0;
+    for (int s = 0; s < b->n; ++s) {
+        const sarbp_grid &g = b->desc[s].grid;
+        const double w = static_cast<double>(g.ny) * g.nz * b->desc[s].num_pulses;
+        pad64 += w * ((g.nx + 63) / 64 * 64);
+        pad32 += w * ((g.nx + 31) / 32 * 32);
+    }
+    const bool tall_tiles = pad64 <= 1.15 * pad32;
     for (const size_t limit : {110u * 1024u, 227u * 1024u})
         for (int i = 0; i < bp_batch_tile_count; ++i) {
             const TileConfig tc = bp_batch_tiles[i];
+            if (tc.mx == 8 && !tall_tiles) continue;
             // quick shared-memory check before configure allocates anything
             int wmax = 0;
             for (int s = 0; s < b->n; ++s) {
@@ -377,9 +388,11 @@ int sarbp_batch_create(const sarbp_plan_desc *descs, int num_scenes, sarbp_batch
         axis(d.grid.ny, d.grid.y0, d.grid.wy, &b->bottom[i], &b->dy[i]);
         axis(d.grid.nz, d.grid.z0, d.grid.wz, &b->zlow[i], &b->dz[i]);
         // rows guarded for the largest tile shape any autotuning may pick
+        int mx_max = 1;
+        for (int t = 0; t < bp_batch_tile_count; ++t) mx_max = bp_batch_tiles[t].mx > mx_max ? bp_batch_tiles[t].mx : mx_max;
         int W, ws;
         double hd;
-        tile_window(b->lambda[i], b->dx[i], b->dy[i], 4, &W, &ws, &hd);
+        tile_window(b->lambda[i], b->dx[i], b->dy[i], mx_max, &W, &ws, &hd);
         b->guard[i] = ws + 2;
         b->row_stride[i] = static_cast<long long>(d.nfft) + 2LL * b->guard[i];
         const size_t np = static_cast<size_t>(d.num_pulses);

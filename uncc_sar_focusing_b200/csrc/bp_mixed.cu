@@ -579,7 +579,7 @@ int bp_mixed_resident(const TileConfig &tc, size_t smem) {
 }
 
 // Tile shapes instantiated for batches; the batch autotuner times these.
-const TileConfig bp_batch_tiles[] = {{4, 8}, {4, 4}, {2, 8}, {2, 4}, {1, 8}, {1, 4}};
+const TileConfig bp_batch_tiles[] = {{8, 8}, {8, 4}, {4, 8}, {4, 4}, {2, 8}, {2, 4}, {1, 8}, {1, 4}};
 const int bp_batch_tile_count = static_cast<int>(sizeof(bp_batch_tiles) / sizeof(bp_batch_tiles[0]));
 
 cudaError_t launch_bp_mixed_batch(const BatchScene *scenes, int nscenes, long long units, long long tiles,
@@ -591,6 +591,8 @@ cudaError_t launch_bp_mixed_batch(const BatchScene *scenes, int nscenes, long lo
 #define SARBP_BATCH_CASE(MX_, PB_) \
     if (tc.mx == MX_ && tc.pb == PB_)  \
         return launch_batch_mx_pb<MX_, PB_>(scenes, nscenes, units, tiles, smem, resident, L0, done, per_tile, s);
+    SARBP_BATCH_CASE(8, 8)
+    SARBP_BATCH_CASE(8, 4)
     SARBP_BATCH_CASE(4, 8)
     SARBP_BATCH_CASE(4, 4)
     SARBP_BATCH_CASE(2, 8)
@@ -604,6 +606,8 @@ cudaError_t launch_bp_mixed_batch(const BatchScene *scenes, int nscenes, long lo
 int bp_mixed_batch_resident(const TileConfig &tc, size_t smem) {
 #define SARBP_BATCH_CASE(MX_, PB_) \
     if (tc.mx == MX_ && tc.pb == PB_) return batch_resident_mx_pb<MX_, PB_>(smem);
+    SARBP_BATCH_CASE(8, 8)
+    SARBP_BATCH_CASE(8, 4)
     SARBP_BATCH_CASE(4, 8)
     SARBP_BATCH_CASE(4, 4)
     SARBP_BATCH_CASE(2, 8)
