@@ -56,8 +56,8 @@ template <int MX, bool GATE, bool NEAR>
 __device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, const float4 *base, uint32_t w_addr,
                                               uint32_t zero_addr, int warp, int lane, float lam,
                                               const float2 (&nd2)[MX], const float2 (&npsi)[MX],
-                                              const float2 (&gm)[MX], float i0f, float j0f, float inv_lam, float2 &T,
-                                              float2 &V, float4 &E) {
+                                              const float2 (&gm)[MX], float i0f, float j0f, float inv_lam, int W,
+                                              float2 &T, float2 &V, float4 &E) {
     const float4 c0 = *reinterpret_cast<const float4 *>(&g.a8r);  // a8r, b1r, g8, e1
     const float4 c1 = *reinterpret_cast<const float4 *>(&g.tx);   // tx, ty, h, hr
     const float4 c2 = *reinterpret_cast<const float4 *>(&g.kr);   // kr, rc, lo, hi
@@ -70,8 +70,9 @@ __device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, const float4 *b
     float2 Bb = make_float2(B00, B00 + c0.w);
     const float2 TX8 = splat(8.0f * c1.x), A8 = splat(c0.x), G8 = splat(c0.z);
     const float2 HR = splat(c1.w), H = splat(c1.z), NKR = splat(-c2.x), NLAM = splat(-lam);
-    const float2 MAGIC = splat(kRoundMagic), NMAGIC = splat(-kRoundMagic), NEG1 = splat(-1.0f);
-    const uint32_t w_adj = w_addr - kRoundMagicBits * 16u;
+    const float2 MAGIC = splat(kRoundMagic);
+    // B is the window-centred bin (entry floor(B) + W, intercept form)
+    const uint32_t w_adj = w_addr + (static_cast<uint32_t>(W) - kRoundMagicBits) * 16u;
     const float nu = c2.x * inv_lam;
 #pragma unroll
     for (int k = 0; k < MX; ++k) {
@@ -96,24 +97,23 @@ __device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, const float4 *b
         const float2 TH = __ffma2_rn(NKR, ng, __fadd2_rn(Pb, npsi[k]));
         const float2 B = __ffma2_rn(NLAM, ng, Bb);
         const float2 y = __fadd2_rd(B, MAGIC);
-        const float2 a = __ffma2_rn(__fadd2_rn(y, NMAGIC), NEG1, B);
         float2 st;  // s~ of the pair
 #pragma unroll
         for (int l = 0; l < 2; ++l) {
             const float Tl = l ? TH.y : TH.x;
             const float yl = l ? y.y : y.x;
-            const float al = l ? a.y : a.x;
+            const float Bl = l ? B.y : B.x;
             float sn, cs;
             __sincosf(Tl, &sn, &cs);
             uint32_t addr = __float_as_uint(yl) * 16u + w_adj;
             if (GATE) {
-                const float Bl = l ? B.y : B.x;
                 const bool valid = (Bl > c2.z) && (Bl < c2.w);
                 addr = valid ? addr : zero_addr;
             }
+            // intercept-form entry {c, v'}: v(B) = c + B v'
             const float4 v = lds128(addr);
-            const float vr = fmaf(al, v.z, v.x);
-            const float vi = fmaf(al, v.w, v.y);
+            const float vr = fmaf(Bl, v.z, v.x);
+            const float vi = fmaf(Bl, v.w, v.y);
             // Z = v' + j nu v; s~ = Re(Z exp(j theta))
             const float zr = fmaf(-nu, vi, v.z);
             const float zi = fmaf(nu, vr, v.w);
@@ -260,6 +260,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                           bar_base + 8 * s, warp, lane, TX / 2, cx, cy, cz);
     };
     produce(0);
+    intercept_slots<PB>(geo, win_addr, bar_base, 0, L.wsize, L.W, warp, lane, L.err);
     __syncthreads();
 
     int last_issued = 0;
@@ -321,7 +322,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                     float4 E;
                     adjoint_pulse<MX, false, false>(geo[s * PB + q], bases + (s * PB + q) * kBaseEntries,
                                                     w0 + q * pulse_bytes, zero_addr, warp, lane, lam, nd2, npsi, gm,
-                                                    i0f, j0f, inv_lam, T, V, E);
+                                                    i0f, j0f, inv_lam, L.W, T, V, E);
                     far_sums(r, T, V);
                 }
             } else if (ok) {
@@ -336,14 +337,14 @@ __global__ void __launch_bounds__(kThreads, 2)
                     float4 E = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                     if (g.flags & PG_NEAR) {
                         adjoint_pulse<MX, true, true>(g, bq, w, zero_addr, warp, lane, lam, nd2, npsi, gm, i0f, j0f,
-                                                      inv_lam, T, V, E);
+                                                      inv_lam, L.W, T, V, E);
                         v[4 * r + 0] = E.x;
                         v[4 * r + 1] = E.y;
                         v[4 * r + 2] = E.z;
                         v[4 * r + 3] = E.w;
                     } else {
                         adjoint_pulse<MX, true, false>(g, bq, w, zero_addr, warp, lane, lam, nd2, npsi, gm, i0f,
-                                                       j0f, inv_lam, T, V, E);
+                                                       j0f, inv_lam, L.W, T, V, E);
                         far_sums(r, T, V);
                     }
                 }
@@ -351,6 +352,10 @@ __global__ void __launch_bounds__(kThreads, 2)
             const float rs = warp_reduce_scatter<NV>(v, lane);
             if ((lane & ((1 << shift) - 1)) == 0) red_s[warp * 4 * PB + gi * NV + (lane >> shift)] = rs;
         }
+        // the next stage's windows into intercept form, published by the barrier
+        if (i + 1 < n)
+            intercept_slots<PB>(geo + (s ^ 1) * PB, win_addr + (s ^ 1) * buf_bytes, bar_base + 8 * (s ^ 1),
+                                ((i + 1) >> 1) & 1, wsize, L.W, warp, lane, L.err);
         if (__syncthreads_or(!ok)) {
             // let the copies already issued for the other buffer land before
             // the CTA's shared memory goes away (again bounded)

@@ -63,7 +63,7 @@ template <int MX, bool GATE, bool NEAR, bool CHECKED>
 __device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, const float4 *base, uint32_t w_addr,
                                                  uint32_t zero_addr, int warp, int lane, float lam,
                                                  const float2 (&nd2)[MX], float (&acc_re)[MX][2],
-                                                 float (&acc_im)[MX][2], int wsize, unsigned *err) {
+                                                 float (&acc_im)[MX][2], int wsize, int W, unsigned *err) {
     const float4 c0 = *reinterpret_cast<const float4 *>(&g.a8r);  // a8r, b1r, g8, e1
     const float4 c1 = *reinterpret_cast<const float4 *>(&g.tx);   // tx, ty, h, hr
     const float4 c2 = *reinterpret_cast<const float4 *>(&g.kr);   // kr, rc, lo, hi
@@ -78,9 +78,10 @@ __device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, const float4
     float2 Bb = make_float2(B00, B00 + c0.w);
     const float2 TX8 = splat(8.0f * c1.x), A8 = splat(c0.x), G8 = splat(c0.z);
     const float2 HR = splat(c1.w), H = splat(c1.z), NKR = splat(-c2.x), NLAM = splat(-lam);
-    const float2 MAGIC = splat(kRoundMagic), NMAGIC = splat(-kRoundMagic), NEG1 = splat(-1.0f);
-    // shared address of pair entry floor(B): bits(B + 1.5*2^23, rounded down) * 16 + w_adj (mod 2^32)
-    const uint32_t w_adj = w_addr - kRoundMagicBits * 16u;
+    const float2 MAGIC = splat(kRoundMagic);
+    // B is the window-centred bin; shared address of pair entry floor(B) + W:
+    // bits(B + 1.5*2^23, rounded down) * 16 + w_adj (mod 2^32)
+    const uint32_t w_adj = w_addr + (static_cast<uint32_t>(W) - kRoundMagicBits) * 16u;
 #pragma unroll
     for (int k = 0; k < MX; ++k) {
         if (k > 0) {
@@ -100,13 +101,11 @@ __device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, const float4
         const float2 P = __ffma2_rn(NKR, ng, Pb);
         const float2 B = __ffma2_rn(NLAM, ng, Bb);
         const float2 y = __fadd2_rd(B, MAGIC);
-        const float2 a = __ffma2_rn(__fadd2_rn(y, NMAGIC), NEG1, B);
 #pragma unroll
         for (int l = 0; l < 2; ++l) {
             const float Pl = l ? P.y : P.x;
             const float Bl = l ? B.y : B.x;
             const float yl = l ? y.y : y.x;
-            const float al = l ? a.y : a.x;
             float sn, cs;
             __sincosf(Pl, &sn, &cs);
             uint32_t addr = __float_as_uint(yl) * 16u + w_adj;
@@ -115,15 +114,16 @@ __device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, const float4
                 addr = valid ? addr : zero_addr;
             }
             if (CHECKED) {
-                const uint32_t idx = __float_as_uint(yl) - kRoundMagicBits;
+                const uint32_t idx = __float_as_uint(yl) - kRoundMagicBits + static_cast<uint32_t>(W);
                 if (idx > static_cast<uint32_t>(wsize - 2)) {
                     atomicOr(err, ERRBIT_BOUNDS);
                     addr = zero_addr;
                 }
             }
+            // intercept-form entry {c, v'}: v(B) = c + B v'
             const float4 v = lds128(addr);
-            const float re = fmaf(al, v.z, v.x);
-            const float im = fmaf(al, v.w, v.y);
+            const float re = fmaf(Bl, v.z, v.x);
+            const float im = fmaf(Bl, v.w, v.y);
             acc_re[k][l] = fmaf(re, cs, fmaf(-im, sn, acc_re[k][l]));
             acc_im[k][l] = fmaf(re, sn, fmaf(im, cs, acc_im[k][l]));
         }
@@ -313,6 +313,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
     };
 
     produce(0);
+    intercept_slots<PB>(geo, win_addr, bar_base, 0, pc.L->wsize, pc.L->W, warp, lane, pc.L->err);
     __syncthreads();
 
     int last_issued = 0;
@@ -342,7 +343,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
                 for (int q = 0; q < PB; ++q)
                     accumulate_pulse<MX, false, false, CHECKED>(geo[s * PB + q], bases + (s * PB + q) * kBaseEntries,
                                                                 w0 + q * pulse_bytes, zero_addr, warp, lane, lam,
-                                                                nd2, acc_re, acc_im, wsize, L.err);
+                                                                nd2, acc_re, acc_im, wsize, L.W, L.err);
             } else {
                 for (int q = 0; q < nq; ++q) {
                     const PulseGeo &g = geo[s * PB + q];
@@ -352,16 +353,20 @@ __global__ void __launch_bounds__(kThreads, MINB)
                     const uint32_t w = w0 + q * pulse_bytes;
                     if (flags & PG_NEAR)
                         accumulate_pulse<MX, true, true, CHECKED>(g, bq, w, zero_addr, warp, lane, lam, nd2, acc_re,
-                                                                  acc_im, wsize, L.err);
+                                                                  acc_im, wsize, L.W, L.err);
                     else if (flags & PG_GATE)
                         accumulate_pulse<MX, true, false, CHECKED>(g, bq, w, zero_addr, warp, lane, lam, nd2, acc_re,
-                                                                   acc_im, wsize, L.err);
+                                                                   acc_im, wsize, L.W, L.err);
                     else
                         accumulate_pulse<MX, false, false, CHECKED>(g, bq, w, zero_addr, warp, lane, lam, nd2,
-                                                                    acc_re, acc_im, wsize, L.err);
+                                                                    acc_re, acc_im, wsize, L.W, L.err);
                 }
             }
         }
+        // the next stage's windows into intercept form, published by the barrier
+        if (i + 1 < n)
+            intercept_slots<PB>(geo + (s ^ 1) * PB, win_addr + (s ^ 1) * buf_bytes, bar_base + 8 * (s ^ 1),
+                                ((i + 1) >> 1) & 1, pc.L->wsize, pc.L->W, warp, lane, L.err);
         if (__syncthreads_or(!ok)) {
             // let the copies already issued for the other buffer land before
             // the CTA's shared memory goes away (again bounded)

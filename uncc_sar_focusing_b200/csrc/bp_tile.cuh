@@ -138,8 +138,9 @@ __device__ __forceinline__ PulseGeo make_geo(const BpLaunch &L, int p, long long
     g.hr = static_cast<float>(0.5 * inv * inv);
     g.kr = static_cast<float>(kTwoPi * k);
     g.rc = static_cast<float>(rc);
-    g.lo = static_cast<float>(-ws);
-    g.hi = static_cast<float>(L.nfft - 1 - ws);
+    // validity bounds of the window-centred bin (bin - ws - W)
+    g.lo = static_cast<float>(-ws - L.W);
+    g.hi = static_cast<float>(L.nfft - 1 - ws - L.W);
     g.ws = ws;
     g.ux = static_cast<float>(ux);
     g.uy = static_cast<float>(uy);
@@ -193,7 +194,7 @@ __device__ __forceinline__ void produce_slots(const BpLaunch &L, int b, PulseGeo
                 const int i0 = lane - tx_half;
                 const double pr = fma(static_cast<double>(i0), alpha, A);
                 tab[32 + lane] = make_float4(static_cast<float>(kTwoPi * (pr - rint(pr))),
-                                             static_cast<float>(fma(static_cast<double>(i0), gam, B0)),
+                                             static_cast<float>(fma(static_cast<double>(i0), gam, B0 - L.W)),
                                              static_cast<float>(i0) * tx, 0.0f);
             }
             __syncwarp();
@@ -220,7 +221,41 @@ __device__ __forceinline__ float4 lds128(uint32_t addr) {
     return v;
 }
 
+__device__ __forceinline__ void sts64(uint32_t addr, float x, float y) {
+    asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(x), "f"(y) : "memory");
+}
+
 __device__ __forceinline__ float2 splat(float a) { return make_float2(a, a); }
+
+// Intercept form of the windows: entry n of a pulse's window holds
+// {v_n, v'_n} (v'_n = v_(n+1) - v_n); rewritten in place to
+// {v_n - (n - W) v'_n, v'_n}, a pixel whose window-centred bin is
+// B = bin - ws - W (floor(B) + W = n) interpolates
+//     v(B) = v_n + (B + W - n) v'_n = c_n + B v'_n
+// with one fused multiply-add and no fraction.  Warp `warp` rewrites the
+// slots it produced (q = warp, warp + 8, ...) of one stage buffer once their
+// copies have landed (bounded wait on the buffer's mbarrier; a timeout sets
+// the error bit and leaves the windows as they are).  The CTA barrier that
+// follows publishes them.
+template <int PB>
+__device__ __forceinline__ void intercept_slots(const PulseGeo *geo_s, uint32_t win_s, uint32_t bar, uint32_t parity,
+                                                int wsize, int W, int warp, int lane, unsigned *err) {
+    if (warp >= PB) return;
+    if (!mbar_wait_bounded(bar, parity, err)) return;
+    for (int q = warp; q < PB; q += kWarps) {
+        if (!(geo_s[q].flags & PG_ACTIVE)) continue;
+        const uint32_t w = win_s + static_cast<uint32_t>(q) * static_cast<uint32_t>(wsize) * 16u;
+        for (int n = lane; n < wsize; n += 32) {
+            const uint32_t a = w + static_cast<uint32_t>(n) * 16u;
+            const float4 e = lds128(a);
+            const float m = static_cast<float>(n - W);
+            sts64(a, fmaf(-m, e.z, e.x), fmaf(-m, e.w, e.y));
+        }
+    }
+    // these generic-proxy stores precede the next bulk copy (async proxy) into
+    // the same buffer, issued after the CTA barrier
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
 
 }  // namespace tile
 }  // namespace sarbp
