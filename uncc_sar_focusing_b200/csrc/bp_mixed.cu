@@ -54,9 +54,10 @@ constexpr int kCtasPerSm = SARBP_CTAS_PER_SM;
 
 
 // One pulse into the thread's MX x 2 pixels.  The two columns l = 0, 1 of a
-// row form a pair and all of their geometry arithmetic runs as paired FP32
-// instructions (__ffma2_rn and friends); the sine/cosine, the shared-memory
-// gather, the interpolation and the complex accumulate are per pixel.
+// row form a pair and their geometry arithmetic and complex
+// multiply-accumulate run as paired FP32 instructions (__ffma2_rn and
+// friends); the sine/cosine, the shared-memory gather and the interpolation
+// are per pixel.
 // Sign conventions avoid negations: nd2 = -|d|^2, so ne = t^2 - |d|^2 = -e,
 // ng = ne (h + t hr) = -g, and the phase / bin add -kr * ng, -lam * ng.
 template <int MX, bool GATE, bool NEAR, bool CHECKED>
@@ -101,6 +102,7 @@ __device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, const float4
         const float2 P = __ffma2_rn(NKR, ng, Pb);
         const float2 B = __ffma2_rn(NLAM, ng, Bb);
         const float2 y = __fadd2_rd(B, MAGIC);
+        float2 RE, IM, CS, SN;  // the pair's interpolated samples and rotations
 #pragma unroll
         for (int l = 0; l < 2; ++l) {
             const float Pl = l ? P.y : P.x;
@@ -124,9 +126,27 @@ __device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, const float4
             const float4 v = lds128(addr);
             const float re = fmaf(Bl, v.z, v.x);
             const float im = fmaf(Bl, v.w, v.y);
-            acc_re[k][l] = fmaf(re, cs, fmaf(-im, sn, acc_re[k][l]));
-            acc_im[k][l] = fmaf(re, sn, fmaf(im, cs, acc_im[k][l]));
+            if (l) {
+                RE.y = re;
+                IM.y = im;
+                CS.y = cs;
+                SN.y = sn;
+            } else {
+                RE.x = re;
+                IM.x = im;
+                CS.x = cs;
+                SN.x = sn;
+            }
         }
+        // complex multiply-accumulate of the pair as paired FP32 (same fused
+        // operations as per pixel, half the instructions)
+        float2 ar = make_float2(acc_re[k][0], acc_re[k][1]), ai = make_float2(acc_im[k][0], acc_im[k][1]);
+        ar = __ffma2_rn(RE, CS, __ffma2_rn(make_float2(-IM.x, -IM.y), SN, ar));
+        ai = __ffma2_rn(RE, SN, __ffma2_rn(IM, CS, ai));
+        acc_re[k][0] = ar.x;
+        acc_re[k][1] = ar.y;
+        acc_im[k][0] = ai.x;
+        acc_im[k][1] = ai.y;
     }
 }
 

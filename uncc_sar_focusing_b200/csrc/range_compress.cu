@@ -203,9 +203,25 @@ __device__ __forceinline__ void rc_fused_body(const float2 *__restrict__ ph, con
     const int tid = threadIdx.x, r = tid >> 5, lane = tid & 31;
     for (int i = tid; i < T::kSize; i += 32 * R) tb[i] = tab[i];
     float2 *reg = regions + r * REG;
+    // a pulse's input samples, loaded one pulse ahead: issued before the
+    // current pulse's row writes (the long phase), consumed after the barrier
+    constexpr int KPT = (K + 32 * R - 1) / (32 * R);
+    float2 pre[KPT];
+    auto prefetch = [&](int q) {
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            const int k = tid + j * 32 * R;
+            pre[j] = (q < np && k < K) ? ph[static_cast<long long>(q) * K + k] : make_float2(0.0f, 0.0f);
+        }
+    };
+    prefetch(blockIdx.x);
     for (int p = blockIdx.x; p < np; p += gridDim.x) {
         __syncthreads();  // the previous pulse's reads of the regions are done; the table is staged
-        for (int k = tid; k < K; k += 32 * R) y[k] = cmulf(ph[static_cast<long long>(p) * K + k], fac[k]);
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            const int k = tid + j * 32 * R;
+            if (k < K) y[k] = cmulf(pre[j], fac[k]);
+        }
         __syncthreads();
         // z[k1 + 32 k2] = y[.] W_N^{k1 r} W_{N/32}^{k2 r}, transformed over k2
         const float2 a = tb[T::kWn + lane * r];
@@ -230,6 +246,7 @@ __device__ __forceinline__ void rc_fused_body(const float2 *__restrict__ ph, con
             for (int m1 = 0; m1 < 32; ++m1) reg[lane + K2 * m1] = w[bit_reverse<32>(m1)];
         }
         __syncthreads();
+        prefetch(p + gridDim.x);
         // rc[R m + r] = regions[r][m]
         float4 *row = pairs + static_cast<long long>(p) * row_stride + guard;
         for (int b = tid - 1; b < N; b += 32 * R) {
