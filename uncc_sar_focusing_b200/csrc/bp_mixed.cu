@@ -19,14 +19,17 @@
 //    bins any pixel of the tile can touch: +-|tile half-diagonal|), so the
 //    FP64 work and the copy issue are spread evenly over the warps;
 //  * range profiles live in HBM as pair entries {rc[b], rc[b+1]-rc[b]}
-//    (float4): one 16-byte shared-memory load and two FMAs interpolate;
+//    (float4); once a window lands its producing warp rewrites it in
+//    shared memory to intercept form {rc[b] - (n - W) slope, slope}, so one
+//    16-byte load and two FMAs on the window-centred bin interpolate;
 //  * per pixel-pulse all arithmetic is FP32: dR = (Rc - R0) - u.d + g with
 //    the FP64 per-tile part carried as a per-thread phase and bin base,
 //    g = e (h + t hr) the far-field remainder (exact sqrt form for near-field
 //    pulses); the phase stays in radians within a few multiples of pi of
-//    zero and goes straight to __sincosf; floor and fraction of the bin come
-//    from one round-down add whose result bits also form the shared-memory
-//    address;
+//    zero and goes straight to __sincosf; the floor of the bin comes from one
+//    round-down add whose result bits also form the shared-memory address;
+//  * MX = 8 (64 x 64-pixel tiles) by default: the per-(tile, pulse) and
+//    per-(thread, pulse) work is spread over 16 pixels per thread;
 //  * complex64 results leave as float4 stores of two adjacent pixels.
 #include <cstdint>
 
