@@ -7,6 +7,11 @@ no distributed mode at all.  `slab_grid` gives rank r its slab as a grid of
 its own, on exactly the pixel positions of the full grid; `gather_slabs`
 assembles the full image on every rank with one all_gather (used when a
 caller wants the whole image; the throughput bench does not gather).
+
+Gradient autofocus on a sharded image has one real exchange per step:
+`sharded_entropy_gradient` all-reduces the image power and sum p log p
+(two scalars) so every rank can form its slab's upstream gradient, runs the
+adjoint on its slab, and all-reduces the 4 Np per-pulse gradients.
 """
 from __future__ import annotations
 
@@ -58,3 +63,41 @@ def gather_slabs(slab, grid: Grid, group=None):
     parts = [torch.empty_like(pad) for _ in range(world)]
     dist.all_gather(parts, pad, group=group)
     return torch.cat([p[..., : b - a] for p, (a, b) in zip(parts, widths)], dim=-1)
+
+
+def sharded_entropy_gradient(slab, adjoint, group=None):
+    """Entropy of the whole image and its gradient with respect to the
+    per-pulse geometry, when every rank holds one slab of the image.
+
+    E = -sum_q p_q log p_q with p_q = |I_q|^2 / S, S = sum_q |I_q|^2 over all
+    ranks' pixels, so dE/d|I_q|^2 = -(log p_q + E) / S and the upstream
+    gradient of pixel q (dE/dRe + j dE/dIm) is G_q = -2 (log p_q + E) I_q / S:
+    after two scalar all-reduces (S and sum p log p) each rank forms G on its
+    own slab.  `adjoint(G)` returns this rank's (grad_ant [3, Np],
+    grad_r0 [Np]) for its slab (e.g. Plan.backproject_adjoint bound to the
+    geometry, or the FP64 oracle); the per-pulse gradients are sums over
+    pixels, so one all-reduce of 4 Np doubles gives the whole image's.
+
+    slab: complex tensor [nz, nx, ny_r].  Returns (E, grad_ant, grad_r0),
+    the same on every rank (float64 tensors on slab's device).  Collectives
+    run on `group` (default: the world); with NCCL, slab lives on this rank's
+    GPU."""
+    import torch
+    import torch.distributed as dist
+
+    w = slab.real.double() ** 2 + slab.imag.double() ** 2
+    S = w.sum().reshape(1)
+    dist.all_reduce(S, group=group)
+    p = w / S
+    logp = torch.log(p.clamp_min(1e-300))
+    plogp = (p * logp).sum().reshape(1)
+    dist.all_reduce(plogp, group=group)
+    E = -plogp
+    G = (-2.0 * (logp + E) / S) * slab.to(torch.complex128)
+    grad_ant, grad_r0 = adjoint(G.to(slab.dtype))
+    grad_ant = torch.as_tensor(grad_ant, dtype=torch.float64, device=slab.device)
+    grad_r0 = torch.as_tensor(grad_r0, dtype=torch.float64, device=slab.device)
+    n = grad_r0.numel()
+    packed = torch.cat([grad_ant.reshape(-1), grad_r0.reshape(-1)])
+    dist.all_reduce(packed, group=group)
+    return E[0], packed[: 3 * n].reshape(3, n), packed[3 * n:]
