@@ -752,6 +752,13 @@ def gpu_arm(args):
         if traffic is not None:
             line["roofline"]["traffic"] = traffic
             line["roofline"]["traffic_source"] = "profiles/bp_mixed_large.md (ncu dram__bytes_read+write, per launch)"
+            # the same kernel against the HBM roofline: profiled DRAM bytes per
+            # launch over this run's CUDA-event time, measured copy bandwidth
+            hbm_ach = traffic / (bp_ms * 1e-3) / 1e9
+            line["roofline"]["hbm"] = {"bound": "hbm", "achieved": hbm_ach, "peak": hbm, "unit": "GB/s",
+                                       "frac": hbm_ach / hbm, "peak_kind": hbm_kind,
+                                       "what": "backprojection kernel's DRAM traffic: it is bound by the MUFU "
+                                               "pipe and issue, not by HBM"}
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_reference_rate(sc, args.cpu_seconds)
             cb.pop("seconds", None)
