@@ -77,24 +77,26 @@ def check_scene(scene, mx):
     return worst_lo, worst_hi, P
 
 
-@pytest.mark.parametrize("mx", [1, 2, 4])
+@pytest.mark.parametrize("mx", [1, 2, 4, 8])
 def test_point_target_config_indices(mx):
     sc = S.point_target_scene(K=424, Np=64, n=256, spacing=0.08, snr_db=None, n_targets=1)
     lo, hi, P = check_scene(sc, mx)
     assert lo >= 1 and hi <= P["wsize"] - 3  # at least one entry of margin on each side
 
 
-def test_large_config_indices():
+@pytest.mark.parametrize("mx", [4, 8])
+def test_large_config_indices(mx):
     sc = S.large_scene(K=64, Np=48, n=1024, n_targets=1)
     sc.nfft = 8 * 1024  # the large configuration's range sampling (max_wr from 640 MHz over 1024 samples)
     sc.delta_freq = 640e6 / 1023
-    check_scene(sc, 4)
+    check_scene(sc, mx)
 
 
 def test_swath_edge_and_odd_grid_indices():
     # scene wider than the swath: tiles whose windows cross the range edges
     sc = S.point_target_scene(K=32, Np=40, n=8, spacing=1.0, nfft=64, snr_db=None, n_targets=1)
     sc.grid = S.Grid(nx=70, ny=45, wx=69 * 0.9, wy=44 * 1.3, x0=3.0, y0=-2.0)
+    check_scene(sc, 8)
     check_scene(sc, 4)
     check_scene(sc, 1)
 
@@ -102,6 +104,7 @@ def test_swath_edge_and_odd_grid_indices():
 def test_near_field_indices():
     sc = S.point_target_scene(K=64, Np=32, n=64, spacing=0.1, nfft=512, snr_db=None, n_targets=1, radius=60.0)
     check_scene(sc, 4)
+    check_scene(sc, 8)
 
 
 # ---- work split of the forward kernels (tile::sk_lo / sk_owner / sk_slot) ----

@@ -125,3 +125,20 @@ def test_plan_info_reports_the_split(F):
         assert info["resident_ctas"] > 0 and info["window_bins"] >= 4
         split = info["tiles"] % info["resident_ctas"] != 0
         assert info["kernels_per_backproject"] == (2 if split else 1)
+
+
+@pytest.mark.parametrize("nx,mx_mixed", [(96, 4), (256, 8), (200, 8), (40, 8)])
+def test_tile_height_follows_row_padding(F, nx, mx_mixed):
+    """Mixed plans take 64-row tiles unless padding the rows to a multiple of
+    64 adds more than 15% over padding to 32 (96 rows: 128 vs 96); FP64
+    plans keep at most 32-row tiles.  Either way the image matches FP64."""
+    sc = S.point_target_scene(K=64, Np=24, n=40, spacing=0.2, nfft=512, snr_db=None, seed=31, n_targets=3,
+                              extent=6.0)
+    sc.grid = S.Grid(nx=nx, ny=48, wx=(nx - 1) * 0.1, wy=47 * 0.1)
+    with F.Plan.for_scene(sc, "mixed") as plan:
+        assert plan.info["tile_mx"] == mx_mixed
+        img = plan.focus(*args(sc))
+    with F.Plan.for_scene(sc, "fp64") as p64:
+        assert p64.info["tile_mx"] <= 4
+        ref = p64.focus(*args(sc))
+    assert O.rel_l2(img, ref) < 1e-4
