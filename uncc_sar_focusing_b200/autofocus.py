@@ -117,10 +117,15 @@ def gradient_autofocus(plan: Plan, motion: CubicMotion, slant_range, start_freq,
     opt = torch.optim.Adam([theta], lr=lr)
     sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, T_max=iters, eta_min=lr / 100.0) if coarse_to_fine \
         else None
-    hist = []
+    # entropies, parameters and completion events stay on the device: no host
+    # read-back inside the loop, so the host queues the next iteration while
+    # the GPU runs this one
+    ents = torch.empty(iters, dtype=torch.float64, device=dev)
+    thetas = torch.empty((iters, 3, 4), dtype=torch.float64, device=dev)
+    events = [torch.cuda.Event(enable_timing=True) for _ in range(iters + 1)]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    best = (float("inf"), theta.detach().clone())
+    events[0].record()
     for it in range(iters):
         opt.zero_grad(set_to_none=True)
         a = motion.track(theta)
@@ -128,16 +133,19 @@ def gradient_autofocus(plan: Plan, motion: CubicMotion, slant_range, start_freq,
                             start_freq)
         E = A.image_entropy(img)
         E.backward()
-        e = float(E.detach())
-        if e < best[0]:
-            best = (e, theta.detach().clone())
+        ents[it] = E.detach()
+        thetas[it] = theta.detach()
+        events[it + 1].record()
         opt.step()
         if sched is not None:
             sched.step()
-        if (log_every and (it % log_every == 0 or it == iters - 1)) or not log_every:
-            hist.append({"iter": it, "entropy": e, "t": time.perf_counter() - t0})
     torch.cuda.synchronize()
-    return AutofocusResult(theta=best[1], history=hist, seconds=time.perf_counter() - t0, images_formed=iters)
+    seconds = time.perf_counter() - t0
+    e_host = ents.cpu().tolist()
+    best = min(range(iters), key=lambda i: e_host[i])
+    hist = [{"iter": it, "entropy": e_host[it], "t": events[0].elapsed_time(events[it + 1]) * 1e-3}
+            for it in range(iters) if (log_every and (it % log_every == 0 or it == iters - 1)) or not log_every]
+    return AutofocusResult(theta=thetas[best].clone(), history=hist, seconds=seconds, images_formed=iters)
 
 
 def grid_search_autofocus(plan: Plan, motion: CubicMotion, slant_range, start_freq, span: float,
@@ -256,22 +264,28 @@ def line_of_sight_autofocus(plan: Plan, ant_x, ant_y, ant_z, slant_range, start_
     slant range tensor, history, seconds)."""
     dr = torch.zeros_like(slant_range, requires_grad=True)
     opt = torch.optim.Adam([dr], lr=lr)
-    hist = []
-    best = (float("inf"), slant_range.detach().clone())
+    ents = torch.empty(iters, dtype=torch.float64, device=slant_range.device)
+    ranges = torch.empty((iters,) + tuple(slant_range.shape), dtype=slant_range.dtype, device=slant_range.device)
+    events = [torch.cuda.Event(enable_timing=True) for _ in range(iters + 1)]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    events[0].record()
     for it in range(iters):
         opt.zero_grad(set_to_none=True)
         r = slant_range + dr
         E = A.image_entropy(A.backproject(plan, ant_x, ant_y, ant_z, r, start_freq))
         E.backward()
-        e = float(E.detach())
-        if e < best[0]:
-            best = (e, r.detach().clone())
+        ents[it] = E.detach()
+        ranges[it] = r.detach()
+        events[it + 1].record()
         opt.step()
-        hist.append({"iter": it, "entropy": e, "t": time.perf_counter() - t0})
     torch.cuda.synchronize()
-    return best[1].contiguous(), hist, time.perf_counter() - t0
+    seconds = time.perf_counter() - t0
+    e_host = ents.cpu().tolist()
+    best = min(range(iters), key=lambda i: e_host[i])
+    hist = [{"iter": it, "entropy": e_host[it], "t": events[0].elapsed_time(events[it + 1]) * 1e-3}
+            for it in range(iters)]
+    return ranges[best].clone().contiguous(), hist, seconds
 
 
 def focus_motion_error(plan: Plan, ant_x, ant_y, ant_z, slant_range, start_freq, cubic_iters: int = 300,
