@@ -96,8 +96,50 @@ def reference_dft_cost(img: torch.Tensor, dyn_range_db: float = 70.0, percentage
     return -float((vals * mask).sum())
 
 
+def _descend(step, iters: int, lr_at, lr: torch.Tensor, record, graph: bool, warm: int = 10):
+    """Run `iters` descent steps; `step()` does one (forward, entropy,
+    backward, optimiser step) on static tensors.  With graph=True the first
+    `warm` steps run eagerly (they initialise the optimiser state and every
+    lazily allocated buffer, and the first steps, where a descent from a
+    metre-scale error gains the most, do not wait for the capture) and the
+    rest replay one CUDA graph captured right after them
+    (capture_begin/capture_end on a side stream: the capture itself executes
+    nothing).  Before step it the learning-rate tensor holds
+    lr_at(it); after it `record(it)` copies the step's outputs on the device.
+    Returns (seconds, completion events; events[0] = start), the events on
+    the GPU clock, the capture included in the wall time."""
+    events = [torch.cuda.Event(enable_timing=True) for _ in range(iters + 1)]
+    cur = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    side = torch.cuda.Stream() if graph else cur
+    side.wait_stream(cur)
+    g = None
+    with torch.cuda.stream(side):
+        events[0].record()
+        for it in range(iters):
+            lr.fill_(lr_at(it))
+            if graph and g is None and it == warm:
+                g = torch.cuda.CUDAGraph()
+                g.capture_begin()
+                step()
+                g.capture_end()
+            if g is not None:
+                g.replay()
+            else:
+                step()
+            record(it)
+            events[it + 1].record()
+    cur.wait_stream(side)
+    torch.cuda.synchronize()
+    seconds = time.perf_counter() - t0
+    del g
+    return seconds, events
+
+
 @dataclasses.dataclass
 class AutofocusResult:
+
     theta: torch.Tensor
     history: List[dict]
     seconds: float
@@ -106,41 +148,46 @@ class AutofocusResult:
 
 def gradient_autofocus(plan: Plan, motion: CubicMotion, slant_range, start_freq, iters: int = 200,
                        lr: float = 0.02, theta0: Optional[torch.Tensor] = None, coarse_to_fine: bool = True,
-                       log_every: int = 1) -> AutofocusResult:
+                       log_every: int = 1, graph: bool = True) -> AutofocusResult:
     """Adam on the 12 coefficients, loss = image entropy, gradient through the
     adjoint backprojection.  With coarse_to_fine the step size decays from
-    `lr` metres to lr/100 (cosine), which lets the first steps cross the
-    large blur of a metre-scale track error and the last ones settle."""
+    `lr` metres to lr/100 (cosine, as CosineAnnealingLR), which lets the first
+    steps cross the large blur of a metre-scale track error and the last ones
+    settle.  Each step is replayed from a captured CUDA graph (graph=False:
+    eager); entropies and parameters stay on the device and the steps are
+    timed with CUDA events, so the host never waits inside the loop."""
     dev = motion.base.device
-    theta = (theta0.clone() if theta0 is not None else torch.zeros((3, 4), dtype=torch.float64, device=dev))
-    theta.requires_grad_(True)
-    opt = torch.optim.Adam([theta], lr=lr)
-    sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, T_max=iters, eta_min=lr / 100.0) if coarse_to_fine \
-        else None
-    # entropies, parameters and completion events stay on the device: no host
-    # read-back inside the loop, so the host queues the next iteration while
-    # the GPU runs this one
-    ents = torch.empty(iters, dtype=torch.float64, device=dev)
-    thetas = torch.empty((iters, 3, 4), dtype=torch.float64, device=dev)
-    events = [torch.cuda.Event(enable_timing=True) for _ in range(iters + 1)]
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    events[0].record()
-    for it in range(iters):
-        opt.zero_grad(set_to_none=True)
+    start = theta0.clone() if theta0 is not None else torch.zeros((3, 4), dtype=torch.float64, device=dev)
+    theta = start.clone().requires_grad_(True)
+    lr_t = torch.tensor(lr, dtype=torch.float64, device=dev)
+    opt = torch.optim.Adam([theta], lr=lr_t, capturable=True)
+    eta_min = lr / 100.0
+
+    def lr_at(it):
+        return eta_min + 0.5 * (lr - eta_min) * (1.0 + math.cos(math.pi * it / iters)) if coarse_to_fine else lr
+
+    e_out = torch.zeros((), dtype=torch.float64, device=dev)
+    theta_pre = torch.zeros_like(start)
+
+    def step():
+        opt.zero_grad(set_to_none=False)
+        theta_pre.copy_(theta.detach())
         a = motion.track(theta)
         img = A.backproject(plan, a[0].contiguous(), a[1].contiguous(), a[2].contiguous(), slant_range,
                             start_freq)
         E = A.image_entropy(img)
         E.backward()
-        ents[it] = E.detach()
-        thetas[it] = theta.detach()
-        events[it + 1].record()
+        e_out.copy_(E.detach())
         opt.step()
-        if sched is not None:
-            sched.step()
-    torch.cuda.synchronize()
-    seconds = time.perf_counter() - t0
+
+    ents = torch.empty(iters, dtype=torch.float64, device=dev)
+    thetas = torch.empty((iters, 3, 4), dtype=torch.float64, device=dev)
+
+    def record(it):
+        ents[it] = e_out
+        thetas[it] = theta_pre
+
+    seconds, events = _descend(step, iters, lr_at, lr_t, record, graph)
     e_host = ents.cpu().tolist()
     best = min(range(iters), key=lambda i: e_host[i])
     hist = [{"iter": it, "entropy": e_host[it], "t": events[0].elapsed_time(events[it + 1]) * 1e-3}
@@ -257,30 +304,36 @@ def pga(img: torch.Tensor, max_iter: int = 30, db_down: float = 30.0, rms_stop: 
 
 
 def line_of_sight_autofocus(plan: Plan, ant_x, ant_y, ant_z, slant_range, start_freq, iters: int = 200,
-                            lr: float = 2e-3) -> tuple:
+                            lr: float = 2e-3, graph: bool = True) -> tuple:
     """Second stage: one slant-range offset per pulse (the line-of-sight part
     of a track error that no low-order polynomial represents, e.g. a random
-    walk), entropy minimised with the adjoint's dL/dR0.  Returns (best
-    slant range tensor, history, seconds)."""
+    walk), entropy minimised with the adjoint's dL/dR0, steps replayed from a
+    captured CUDA graph as in gradient_autofocus.  Returns (best slant range
+    tensor, history, seconds)."""
+    dev = slant_range.device
     dr = torch.zeros_like(slant_range, requires_grad=True)
-    opt = torch.optim.Adam([dr], lr=lr)
-    ents = torch.empty(iters, dtype=torch.float64, device=slant_range.device)
-    ranges = torch.empty((iters,) + tuple(slant_range.shape), dtype=slant_range.dtype, device=slant_range.device)
-    events = [torch.cuda.Event(enable_timing=True) for _ in range(iters + 1)]
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    events[0].record()
-    for it in range(iters):
-        opt.zero_grad(set_to_none=True)
+    lr_t = torch.tensor(lr, dtype=torch.float64, device=dev)
+    opt = torch.optim.Adam([dr], lr=lr_t, capturable=True)
+    e_out = torch.zeros((), dtype=torch.float64, device=dev)
+    r_pre = torch.zeros_like(slant_range)
+
+    def step():
+        opt.zero_grad(set_to_none=False)
         r = slant_range + dr
+        r_pre.copy_(r.detach())
         E = A.image_entropy(A.backproject(plan, ant_x, ant_y, ant_z, r, start_freq))
         E.backward()
-        ents[it] = E.detach()
-        ranges[it] = r.detach()
-        events[it + 1].record()
+        e_out.copy_(E.detach())
         opt.step()
-    torch.cuda.synchronize()
-    seconds = time.perf_counter() - t0
+
+    ents = torch.empty(iters, dtype=torch.float64, device=dev)
+    ranges = torch.empty((iters,) + tuple(slant_range.shape), dtype=slant_range.dtype, device=dev)
+
+    def record(it):
+        ents[it] = e_out
+        ranges[it] = r_pre
+
+    seconds, events = _descend(step, iters, lambda it: lr, lr_t, record, graph)
     e_host = ents.cpu().tolist()
     best = min(range(iters), key=lambda i: e_host[i])
     hist = [{"iter": it, "entropy": e_host[it], "t": events[0].elapsed_time(events[it + 1]) * 1e-3}
