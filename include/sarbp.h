@@ -62,7 +62,7 @@ enum {
     SARBP_OK = 0,
     SARBP_ERR_INVALID_ARGUMENT = 1, /* a size, flag or grid value is out of range */
     SARBP_ERR_NULL_POINTER = 2,     /* a required pointer is NULL */
-    SARBP_ERR_UNSUPPORTED = 3,      /* valid request this build cannot serve */
+    SARBP_ERR_UNSUPPORTED = 3,      /* valid request this library version cannot serve */
     SARBP_ERR_OUT_OF_MEMORY = 4,    /* a device or host allocation failed */
     SARBP_ERR_CUDA = 5,             /* a CUDA runtime call failed */
     SARBP_ERR_CUFFT = 6,            /* a cuFFT call failed */
