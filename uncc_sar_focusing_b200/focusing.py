@@ -412,3 +412,29 @@ def focus_scene(scene: Scene, precision: str = "mixed") -> np.ndarray:
     with Plan.for_scene(scene, precision) as plan:
         return plan.focus(scene.phase_history, scene.ant_x, scene.ant_y, scene.ant_z, scene.slant_range,
                           scene.start_freq)
+
+
+def polar_format_phase_history(phase_history, chirp_rate, adc_rate: float, center_freq: float):
+    """The reference's polar-format algorithm is backprojection of a phase
+    history whose pulses are first modulated (matlab/focusalg_PF.m:33-35; the
+    rest of that file is focusalg_BP's): pulse p of Np is multiplied by
+    exp(-2j pi s_pk / Np) with frequency scales
+    s_pk = 1 + (chirp_rate_p / (adc_rate * center_freq)) (k - K/2), k = 0..K-1
+    (matlab/formSARImage.m:217-220,341, where the degree-to-radian factors of
+    the chirp rate and centre frequency cancel).  Returns the modulated phase
+    history ([Np, K] complex64, numpy array or torch tensor like the input);
+    focus it with Plan.focus / sarbp_focus as any other.
+
+    chirp_rate: per-pulse chirp rates [Np] (or one value), in the units of
+    adc_rate * center_freq (Sandia: ChirpRate, ADF, DesCntrFreq)."""
+    np_, K = int(phase_history.shape[0]), int(phase_history.shape[1])
+    rates = np.broadcast_to(np.asarray(chirp_rate, dtype=np.float64), (np_,))
+    k = np.arange(K, dtype=np.float64) - K / 2.0
+    scales = 1.0 + (rates[:, None] / (adc_rate * center_freq)) * k[None, :]
+    mod = np.exp((-2j * np.pi / np_) * scales)
+    if isinstance(phase_history, np.ndarray):
+        return (phase_history.astype(np.complex128) * mod).astype(np.complex64)
+    import torch
+
+    m = torch.as_tensor(mod, dtype=torch.complex128, device=phase_history.device)
+    return (phase_history.to(torch.complex128) * m).to(torch.complex64)
