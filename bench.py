@@ -74,6 +74,9 @@ def parse_args():
                     help="one warm-up and one focus step of the workload, then two adjoint calls (mixed), "
                          "nothing else (for ncu captures)")
     ap.add_argument("--pulses", type=int, default=0, help="use only the first N pulses (profiling)")
+    ap.add_argument("--profile-reference", action="store_true",
+                    help="the reference's own GPU kernels on the workload, one untimed and one timed run, "
+                         "nothing else (for ncu captures)")
     ap.add_argument("--profile-precision", choices=["mixed", "fp64"], default="mixed",
                     help="engine precision of the --profile run")
     return ap.parse_args()
@@ -816,12 +819,29 @@ def profile_arm(args):
     return 0
 
 
+def profile_reference_arm(args):
+    """The reference's GPU kernels (oracle/_ref/libref_gpu.so) on the
+    workload: scene synthesis, then one untimed and one timed repetition."""
+    import torch
+
+    from oracle import oracle as O
+
+    torch.cuda.set_device(0)
+    sc, _ = make_scene(args.config, 0, 1, "cuda")
+    torch.cuda.empty_cache()
+    _, fft_ms, bp_ms = O.reference_gpu_focus(sc, reps=1)
+    print(json.dumps({"profile_reference": args.config, "bp_ms": bp_ms, "range_compress_ms": fft_ms}))
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return reference_arm(args)
     if args.profile:
         return profile_arm(args)
+    if args.profile_reference:
+        return profile_reference_arm(args)
     return gpu_arm(args)
 
 
