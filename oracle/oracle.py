@@ -1,10 +1,13 @@
 """TEST INFRASTRUCTURE (the oracle), not product code.
 
 ctypes binding of oracle/liboracle.so (the project's CPU restatement of the
-reference backprojection, oracle/bp_oracle.c) and of oracle/_ref/libref_bp*.so
-(the reference's own run_bp compiled from its sources by oracle/Makefile).
-Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
-this module, and only as the checker.
+reference backprojection, oracle/bp_oracle.c), of oracle/_ref/libref_bp*.so
+(the reference's own run_bp compiled from its sources by oracle/Makefile) and
+of oracle/_ref/libref_gpu.so (the reference's own GPU kernels, built from
+their header by the same Makefile, launched by oracle/ref_gpu_harness.cu).
+Only tests/, __graft_entry__.smoke() and bench.py's reference legs (the CPU
+baseline, the reference arm, the reference-GPU timing) import this module:
+as the checker, or as the reference being timed, never as the product.
 """
 from __future__ import annotations
 
