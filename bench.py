@@ -109,15 +109,19 @@ class ClockSampler:
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_id: str):
-        self.path = tempfile.mktemp(suffix=".csv")
         self.proc = None
         try:
-            self.fh = open(self.path, "w")
+            self.fh = tempfile.NamedTemporaryFile("w", suffix=".csv", delete=False)
+            self.path = self.fh.name
             self.proc = subprocess.Popen(["nvidia-smi", "-i", gpu_id, f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            fh = getattr(self, "fh", None)
+            if fh is not None:
+                fh.close()
+                os.unlink(fh.name)
 
     def stop(self):
         if self.proc is None:
