@@ -26,6 +26,15 @@ def test_library_exports_every_declared_entry_point():
     assert set(names) <= set(N.EXPORTED)
 
 
+def test_bindings_mirror_the_header_abi_version():
+    import re
+
+    from uncc_sar_focusing_b200 import _native as N
+
+    hdr = open(os.path.join(ROOT, "include", "sarbp.h")).read()
+    assert int(re.search(r"#define SARBP_ABI_VERSION (\d+)", hdr).group(1)) == N.ABI_VERSION
+
+
 def test_abi_version_and_status_strings():
     lib = N.lib()
     assert lib.sarbp_abi_version() == 1

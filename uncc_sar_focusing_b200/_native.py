@@ -10,6 +10,7 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libsarbp.so")
+ABI_VERSION = 1  # SARBP_ABI_VERSION of the include/sarbp.h these structures mirror
 COMPAT_PATH = os.path.join(HERE, "lib", "libsarbp_compat.so")
 
 SARBP_OK = 0
@@ -92,6 +93,9 @@ def lib():
         L = ctypes.CDLL(LIB_PATH)
         vp, i, P = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER
         L.sarbp_abi_version.restype = i
+        if L.sarbp_abi_version() != ABI_VERSION:
+            raise RuntimeError(f"{LIB_PATH} has ABI version {L.sarbp_abi_version()}, these bindings mirror "
+                               f"version {ABI_VERSION} (include/sarbp.h): rebuild the library")
         L.sarbp_status_string.restype = ctypes.c_char_p
         L.sarbp_status_string.argtypes = [i]
         L.sarbp_plan_create.argtypes = [P(PlanDesc), P(vp)]
