@@ -61,7 +61,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["large", "point_targets"], default="large")
+    ap.add_argument("--config", choices=["large", "point_targets", "volumetric"], default="large")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-autofocus", action="store_true")
@@ -91,6 +91,10 @@ def make_scene(config: str, rank: int, world: int, device):
         sc = S.large_scene(device=device)
         desc = ("large: 1024 samples x 2048 pulses complex64, fc 9.6 GHz / 640 MHz, 30 deg at 8 km, 45 deg el, "
                 "2000 Rayleigh scatterers, 1024x1024 image over 100 m, Nfft 8192")
+    elif config == "volumetric":
+        sc = S.volumetric_scene(device=device)
+        desc = ("volumetric: 8 passes x 1024 pulses x 512 samples, 360 deg azimuth, el 30.0-31.4 deg, 500 "
+                "Rayleigh scatterers on facets in a 10 m cube, 256x256x64 voxels, Nfft 4096")
     else:
         sc = S.point_target_scene(device=device)
         desc = ("point_targets: 424 samples x 512 pulses complex64, fc 9.6 GHz / 600 MHz, 4 deg at 10 km, "

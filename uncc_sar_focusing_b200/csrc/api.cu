@@ -226,7 +226,6 @@ BpLaunch launch_params(const sarbp_plan *p, const double *ax, const double *ay, 
     L.near_coef = p->near_coef;
     L.img = img;
     L.accumulate = (flags & SARBP_ACCUMULATE) ? 1 : 0;
-    L.vec_store = ((reinterpret_cast<uintptr_t>(img) & 15u) == 0 && (g.ny % 2) == 0) ? 1 : 0;
     L.err = p->d_err;
     L.nhyp = 1;
     L.sk_partial = p->d_sk;

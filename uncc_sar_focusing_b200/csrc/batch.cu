@@ -222,7 +222,6 @@ int fill_table(sarbp_batch *b, const sarbp_aperture *aps, void *const *images) {
         L.near_coef = b->near_coef[i];
         L.img = images[i];
         L.accumulate = 0;
-        L.vec_store = ((reinterpret_cast<uintptr_t>(images[i]) & 15u) == 0 && (d.grid.ny % 2) == 0) ? 1 : 0;
         L.err = b->d_err;
         L.nhyp = 1;
         T.fused = b->rctab[i] ? 1 : 0;

@@ -58,14 +58,14 @@ __device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, const float4 *b
                                               const float2 (&nd2)[MX], const float2 (&npsi)[MX],
                                               const float2 (&gm)[MX], float i0f, float j0f, float inv_lam, int W,
                                               float2 &T, float2 &V, float4 &E) {
-    const float4 c0 = *reinterpret_cast<const float4 *>(&g.a8r);  // a8r, b1r, g8, e1
+    const float4 c0 = *reinterpret_cast<const float4 *>(&g.a8r);  // a8r, b32r, g8, e32
     const float4 c1 = *reinterpret_cast<const float4 *>(&g.tx);   // tx, ty, h, hr
     const float4 c2 = *reinterpret_cast<const float4 *>(&g.kr);   // kr, rc, lo, hi
     const float4 rowv = base[32 + warp], colv = base[lane];
     const float P00 = rowv.x + colv.x;
     const float B00 = rowv.y + colv.y;
     const float t00 = rowv.z + colv.z;
-    float2 t2 = make_float2(t00, t00 + c1.y);
+    float2 t2 = make_float2(t00, fmaf(32.0f, c1.y, t00));  // second pixel: 32 columns on
     float2 Pb = make_float2(P00, P00 + c0.y);
     float2 Bb = make_float2(B00, B00 + c0.w);
     const float2 TX8 = splat(8.0f * c1.x), A8 = splat(c0.x), G8 = splat(c0.z);
@@ -131,7 +131,7 @@ __device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, const float4 *b
                 const float sr = s * r;
                 E.x += s;
                 E.y = fmaf(sr, ik, E.y);
-                E.z = fmaf(sr, j0f + static_cast<float>(l), E.z);
+                E.z = fmaf(sr, j0f + static_cast<float>((kTY / 2) * l), E.z);
                 E.w = fmaf(s, c2.y * (r - 1.0f), E.w);
             }
         } else {
@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i0 = warp - TX / 2;
-    const int j0 = 2 * lane - kTY / 2;
+    const int j0 = lane - kTY / 2;  // columns lane and lane + 32 of the tile
     const float i0f = static_cast<float>(i0), j0f = static_cast<float>(j0);
     const float lam = static_cast<float>(L.lambda), inv_lam = static_cast<float>(1.0 / L.lambda);
     const float dxf = static_cast<float>(L.dx), dyf = static_cast<float>(L.dy);
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
     for (int k = 0; k < MX; ++k) {
         const float di = static_cast<float>(i0 + 8 * k) * dxf;
-        const float dj0 = j0f * dyf, dj1 = static_cast<float>(j0 + 1) * dyf;
+        const float dj0 = j0f * dyf, dj1 = static_cast<float>(j0 + kTY / 2) * dyf;
         nd2[k] = make_float2(-fmaf(di, di, dj0 * dj0), -fmaf(di, di, dj1 * dj1));
     }
 
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             float ps[2], mg[2];
 #pragma unroll
             for (int l = 0; l < 2; ++l) {
-                const int col = ty0 + 2 * lane + l;
+                const int col = ty0 + lane + (kTY / 2) * l;
                 const float2 q = (row < L.nx && col < L.ny)
                                      ? grad[(static_cast<long long>(cc.iz) * L.nx + row) * L.ny + col]
                                      : make_float2(0.0f, 0.0f);
@@ -306,13 +306,13 @@ __global__ void __launch_bounds__(kThreads, 2)
             float v[NV];
 #pragma unroll
             for (int c = 0; c < NV; ++c) v[c] = 0.0f;
-            // far field: E0, Ei = i0 E0 + 8 sum k s^, Ej = j0 E0 + sum_(l=1) s^, Et later
+            // far field: E0, Ei = i0 E0 + 8 sum k s^, Ej = j0 E0 + 32 sum_(l=1) s^, Et later
             auto far_sums = [&](int r, float2 T, float2 V) {
                 const float S = T.x + T.y;
                 const float Sk = fmaf(static_cast<float>(MX - 1), S, -(V.x + V.y));
                 v[4 * r + 0] = S;
                 v[4 * r + 1] = fmaf(i0f, S, 8.0f * Sk);
-                v[4 * r + 2] = fmaf(j0f, S, T.y);
+                v[4 * r + 2] = fmaf(j0f, S, static_cast<float>(kTY / 2) * T.y);
             };
             if (fast) {
 #pragma unroll

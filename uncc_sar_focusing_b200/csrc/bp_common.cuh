@@ -113,7 +113,7 @@ struct __align__(16) PulseGeo {
     double A, alpha;   // frac(k (Rc - R0)); frac(-k ux dx): revolutions per x step
     double beta, B0;   // frac(-k uy dy); tile-centre bin relative to the window start
     double gam, eta;   // -lambda ux dx, -lambda uy dy: bins per x / y step
-    float a8r, b1r, g8, e1;  // 2 pi frac(8 alpha), 2 pi beta (rad); 8 gam, eta (bins)
+    float a8r, b32r, g8, e32;  // 2 pi frac(8 alpha), 2 pi frac(32 beta) (rad); 8 gam, 32 eta (bins)
     float tx, ty, h, hr;     // ux dx, uy dy (m); 1/(2 Rc), 1/(2 Rc^2)
     float kr, rc, lo, hi;    // 2 pi k (rad/m); Rc; valid iff lo < B_rel < hi
     int ws;                  // window start bin (may be negative: guard band)

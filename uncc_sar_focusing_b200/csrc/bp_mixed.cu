@@ -10,7 +10,8 @@
 //     GPU kernel's roundf bracket, cuda_BackProjectionKernels.cuh:68-74).
 //
 // Design (one CTA = one pixel tile of (8*MX) x 64 pixels of one z-slice,
-// 256 threads = 8 warps, each thread MX rows (8 apart) x 2 adjacent columns):
+// 256 threads = 8 warps, each thread MX rows (8 apart) x 2 columns (lane and
+// lane + 32, so the lanes of one gather are one column apart):
 //  * pulses go through shared memory in stages of PB pulses, two stages, one
 //    mbarrier per stage with PB arrivals.  For each pulse slot of the next
 //    stage one warp (slot mod 8) computes the (tile, pulse) geometry record in
@@ -68,16 +69,17 @@ __device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, const float4
                                                  uint32_t zero_addr, int warp, int lane, float lam,
                                                  const float2 (&nd2)[MX], float (&acc_re)[MX][2],
                                                  float (&acc_im)[MX][2], int wsize, int W, unsigned *err) {
-    const float4 c0 = *reinterpret_cast<const float4 *>(&g.a8r);  // a8r, b1r, g8, e1
+    const float4 c0 = *reinterpret_cast<const float4 *>(&g.a8r);  // a8r, b32r, g8, e32
     const float4 c1 = *reinterpret_cast<const float4 *>(&g.tx);   // tx, ty, h, hr
     const float4 c2 = *reinterpret_cast<const float4 *>(&g.kr);   // kr, rc, lo, hi
     // per-thread phase, bin and projection bases: row part + column part,
-    // each reduced in FP64 by the producer (|phase| <= 2 pi)
+    // each reduced in FP64 by the producer (|phase| <= 2 pi); the pair's
+    // second pixel is 32 columns on
     const float4 rowv = base[32 + warp], colv = base[lane];
     const float P00 = rowv.x + colv.x;
     const float B00 = rowv.y + colv.y;
     const float t00 = rowv.z + colv.z;
-    float2 t2 = make_float2(t00, t00 + c1.y);
+    float2 t2 = make_float2(t00, fmaf(32.0f, c1.y, t00));
     float2 Pb = make_float2(P00, P00 + c0.y);
     float2 Bb = make_float2(B00, B00 + c0.w);
     const float2 TX8 = splat(8.0f * c1.x), A8 = splat(c0.x), G8 = splat(c0.z);
@@ -154,7 +156,8 @@ __device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, const float4
 }
 
 // Store (or add, L.accumulate) a thread's MX x 2 pixels of the tile at
-// (tx0, ty0, slice zz) into the complex64 image.
+// (tx0, ty0, slice zz) into the complex64 image: columns lane and lane + 32,
+// so every store of a warp is 32 consecutive pixels.
 template <int MX>
 __device__ __forceinline__ void store_pixels(const BpLaunch &L, int tx0, int ty0, int zz, int warp, int lane,
                                              const float (&re)[MX][2], const float (&im)[MX][2]) {
@@ -162,43 +165,25 @@ __device__ __forceinline__ void store_pixels(const BpLaunch &L, int tx0, int ty0
 #pragma unroll
     for (int k = 0; k < MX; ++k) {
         const int row = tx0 + warp + 8 * k;
-        const int col = ty0 + 2 * lane;
-        if (row >= L.nx || col >= L.ny) continue;
-        const long long o = (static_cast<long long>(zz) * L.nx + row) * L.ny + col;
-        if (L.vec_store && col + 1 < L.ny) {
-            float4 v = make_float4(re[k][0], im[k][0], re[k][1], im[k][1]);
-            float4 *dst = reinterpret_cast<float4 *>(img + o);
-            if (L.accumulate) {
-                const float4 old = *dst;
-                v.x += old.x;
-                v.y += old.y;
-                v.z += old.z;
-                v.w += old.w;
-            }
-            *dst = v;
-        } else {
-            float2 v0 = make_float2(re[k][0], im[k][0]);
+        if (row >= L.nx) continue;
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            const int col = ty0 + lane + (kTY / 2) * l;
+            if (col >= L.ny) continue;
+            const long long o = (static_cast<long long>(zz) * L.nx + row) * L.ny + col;
+            float2 v = make_float2(re[k][l], im[k][l]);
             if (L.accumulate) {
                 const float2 old = img[o];
-                v0.x += old.x;
-                v0.y += old.y;
+                v.x += old.x;
+                v.y += old.y;
             }
-            img[o] = v0;
-            if (col + 1 < L.ny) {
-                float2 v1 = make_float2(re[k][1], im[k][1]);
-                if (L.accumulate) {
-                    const float2 old = img[o + 1];
-                    v1.x += old.x;
-                    v1.y += old.y;
-                }
-                img[o + 1] = v1;
-            }
+            img[o] = v;
         }
     }
 }
 
-// Tile-local index of pixel pair (row warp + 8k, columns 2 lane, 2 lane + 1)
-// in a partial-sum slot of TX x 64 complex64 values.
+// Index of thread (warp, lane)'s pixel pair of row group k in a partial-sum
+// slot of TX x 64 complex64 values (written and read by the same mapping).
 __device__ __forceinline__ int slot_pair(int warp, int lane, int k) { return (warp + 8 * k) * kTY + 2 * lane; }
 
 // Unit cursor over one launch (BATCH = false: the kernel parameter's scene)
@@ -281,7 +266,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
     }
     if (n <= 0) return;
     const int i0 = warp - TX / 2;
-    const int j0 = 2 * lane - kTY / 2;
+    const int j0 = lane - kTY / 2;  // column offset of the first pixel (the second is 32 on)
 
     SceneCursor<TX, PB, BATCH> cc, pc;  // consumer at unit i, producer at unit i + 1
     cc.init(&L0, scenes, nscenes, lo);
@@ -301,7 +286,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
 #pragma unroll
         for (int k = 0; k < MX; ++k) {
             const float di = static_cast<float>(i0 + 8 * k) * dxf;
-            const float dj0 = static_cast<float>(j0) * dyf, dj1 = static_cast<float>(j0 + 1) * dyf;
+            const float dj0 = static_cast<float>(j0) * dyf, dj1 = static_cast<float>(j0 + kTY / 2) * dyf;
             nd2[k] = make_float2(-fmaf(di, di, dj0 * dj0), -fmaf(di, di, dj1 * dj1));
         }
     };

@@ -129,9 +129,9 @@ __device__ __forceinline__ PulseGeo make_geo(const BpLaunch &L, int p, long long
     g.gam = -L.lambda * ux * L.dx;
     g.eta = -L.lambda * uy * L.dy;
     g.a8r = static_cast<float>(kTwoPi * frac_rev(8.0 * al));
-    g.b1r = static_cast<float>(kTwoPi * be);
+    g.b32r = static_cast<float>(kTwoPi * frac_rev(32.0 * be));
     g.g8 = static_cast<float>(8.0 * g.gam);
-    g.e1 = static_cast<float>(g.eta);
+    g.e32 = static_cast<float>(32.0 * g.eta);
     g.tx = static_cast<float>(ux * L.dx);
     g.ty = static_cast<float>(uy * L.dy);
     g.h = static_cast<float>(0.5 * inv);
@@ -158,7 +158,8 @@ __device__ __forceinline__ PulseGeo make_geo(const BpLaunch &L, int p, long long
 // lane 0 writes the geometry record and either arrives with the window's byte
 // count and issues its bulk copy, or just arrives (inactive / past the end).
 // Per-(tile, pulse) base tables of the mixed forward kernel: entry lane
-// (0..31) is the column part for j0 = 2 lane - 32 and entry 32 + warp (0..7)
+// (0..31) is the column part for j0 = lane - 32 (a lane's pixels are columns
+// lane and lane + 32 of the tile) and entry 32 + warp (0..7)
 // the row part for i0 = warp - TX/2 of the thread's phase, bin and
 // projection bases: (2 pi frac(j0 beta), j0 eta, j0 ty, 0) and
 // (2 pi frac(A + i0 alpha), B0 + i0 gam, i0 tx, 0), the phase parts reduced
@@ -186,7 +187,7 @@ __device__ __forceinline__ void produce_slots(const BpLaunch &L, int b, PulseGeo
             const double gam = __shfl_sync(full, g.gam, 0), eta = __shfl_sync(full, g.eta, 0);
             const float tx = __shfl_sync(full, g.tx, 0), ty = __shfl_sync(full, g.ty, 0);
             float4 *tab = base_s + q * kBaseEntries;
-            const int j0 = 2 * lane - kTY / 2;
+            const int j0 = lane - kTY / 2;
             const double pc = static_cast<double>(j0) * beta;
             tab[lane] = make_float4(static_cast<float>(kTwoPi * (pc - rint(pc))), static_cast<float>(j0 * eta),
                                     static_cast<float>(j0) * ty, 0.0f);

@@ -186,7 +186,6 @@ extern "C" SARBP_API int sarbp_backproject_noalloc(const sarbp_plan_desc *desc, 
         L.near_coef = 0.625 * hd * hd * hd * hd / 1.0e-7;
         L.img = image;
         L.accumulate = (flags & SARBP_ACCUMULATE) ? 1 : 0;
-        L.vec_store = ((reinterpret_cast<uintptr_t>(image) & 15u) == 0 && (g.ny % 2) == 0) ? 1 : 0;
         L.err = err;
         L.nhyp = 1;
         e = launch_bp_mixed(L, tc, false, smem, s);

@@ -27,7 +27,6 @@ struct BpLaunch {
     double near_coef;       // 0.625 * hd^4 / tolerance (revolutions)
     void *img;              // complex64 / complex128 [nz][nx][ny]
     int accumulate;
-    int vec_store;          // 16-byte aligned image and even ny
     unsigned *err;
     int nhyp;               // geometry hypotheses (mixed forward kernel): arrays [nhyp][np], images [nhyp][nz][nx][ny]
     // Work split of the forward kernels.  The (tile, pulse-stage) units of a
