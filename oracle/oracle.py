@@ -342,3 +342,34 @@ def peak_phase_error(a: np.ndarray, b: np.ndarray) -> float:
     b = np.asarray(b)
     i = int(np.argmax(np.abs(b).ravel()))
     return float(abs(np.angle(np.asarray(a).ravel()[i] * np.conj(b.ravel()[i]))))
+
+
+def pga_step_reference(img: np.ndarray, db_down: float = 30.0) -> np.ndarray:
+    """One iteration of the reference's PGA (matlab/PGA.m:150-212), restated
+    with its 1-based MATLAB indexing written out, in double: the estimated,
+    detrended azimuth phase error phi_error_est_detrended [Nx] of an image
+    [Ny range lines][Nx azimuth samples]."""
+    img = np.asarray(img, dtype=np.complex128)
+    ny, nx = img.shape
+    c = int(np.ceil(nx / 2.0))  # center_az_idx (1-based), :150
+    f = np.zeros_like(img)
+    for row in range(ny):  # :157-164
+        m = int(np.argmax(np.abs(img[row]))) + 1  # 1-based max index
+        f[row] = np.roll(img[row], 1 + c - m)  # circshift(img_af(row,:), 1 + c - m)
+    avg = np.sum(np.conj(img) * img, axis=0).real  # :167
+    avg_db = 10.0 * np.log10(avg / avg.max())
+    cutoff = avg_db.max() - abs(db_down)
+    left_part = np.nonzero(avg_db[:c] - cutoff < 0)[0]  # 1..c (1-based)
+    right_part = np.nonzero(avg_db[c:] - cutoff < 0)[0]  # c+1..end
+    leftidx = (left_part[-1] + 1) + 1 if left_part.size else 1  # 1-based, :172-177
+    rightidx = (right_part[0] + 1) + c - 1 if right_part.size else nx
+    mask = np.zeros(nx)
+    mask[leftidx - 1:rightidx] = 1.0  # window_mask_row(leftidx:rightidx) = 1
+    g = f * mask[None, :]
+    G = np.fft.fft(np.fft.ifftshift(g, axes=1), axis=1)  # :195-196
+    G_dot = np.diff(G, axis=1)
+    phi_dot = np.sum(np.imag(np.conj(G[:, :-1]) * G_dot), axis=0) / np.sum(np.abs(G[:, :-1]) ** 2, axis=0)
+    phi = np.unwrap(np.concatenate([[0.0], np.cumsum(phi_dot)]))  # :204
+    x = np.arange(nx, dtype=np.float64)
+    coeffs = np.polyfit(x, phi, 1)  # :209-212
+    return phi - (coeffs[0] * x + coeffs[1])

@@ -37,6 +37,17 @@ def test_pga_restores_an_injected_phase_error(focused):
     assert rms[-1] < rms[0]
 
 
+@pytest.mark.parametrize("n", [64, 63])
+def test_pga_iteration_matches_the_reference_steps(focused, n):
+    """One PGA iteration's phase estimate equals an independent numpy
+    restatement of matlab/PGA.m:150-212 (1-based indexing written out), on an
+    even and an odd azimuth length."""
+    bad = defocus(focused)[:, :n].contiguous()
+    _, phi, _ = AF.pga(bad, max_iter=1)
+    want = O.pga_step_reference(bad.numpy())
+    assert np.abs(phi.numpy() - want).max() < 1e-5, np.abs(phi.numpy() - want).max()
+
+
 def test_focus_metrics_rank_focus(focused):
     bad = defocus(focused, seed=3)
     assert float(AF.entropy(focused)) < float(AF.entropy(bad))

@@ -258,14 +258,16 @@ def pga(img: torch.Tensor, max_iter: int = 30, db_down: float = 30.0, rms_stop: 
     if az_axis not in (-1, x.dim() - 1):
         x = x.transpose(az_axis, -1)
     rows, n = x.shape[-2], x.shape[-1]
-    center = (n + 1) // 2 - 1  # MATLAB ceil(n/2), 0-based
+    c = (n + 1) // 2  # MATLAB center_az_idx = ceil(n/2) (1-based)
+    center = c - 1  # its 0-based index: the window splits at [0, c) / [c, n)
     col = torch.arange(n, device=x.device)
     total = torch.zeros(n, dtype=torch.float64, device=x.device)
     rms_hist = []
     for _ in range(max_iter):
-        # brightest azimuth sample of each range line to the centre (:159-164)
+        # brightest azimuth sample of each range line to 0-based index c:
+        # circshift(row, 1 + c - m) with m the 1-based peak (:159-164)
         peak = torch.argmax(x.abs(), dim=-1)
-        idx = (col[None, :] - (center - peak)[:, None]) % n
+        idx = (col[None, :] - (c - peak)[:, None]) % n
         f = torch.gather(x, -1, idx)
         # -30 dB window from the non-coherent average of the image (:167-188)
         avg = (x.real ** 2 + x.imag ** 2).sum(dim=0)
