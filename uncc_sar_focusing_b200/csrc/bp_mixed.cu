@@ -31,7 +31,7 @@
 //    round-down add whose result bits also form the shared-memory address;
 //  * MX = 8 (64 x 64-pixel tiles) by default: the per-(tile, pulse) and
 //    per-(thread, pulse) work is spread over 16 pixels per thread;
-//  * complex64 results leave as float4 stores of two adjacent pixels.
+//  * complex64 results leave as float2 stores, 32 consecutive pixels per warp.
 #include <cstdint>
 
 #include "bp_common.cuh"
@@ -57,7 +57,7 @@ constexpr int kFastUnroll = SARBP_FAST_UNROLL;
 constexpr int kCtasPerSm = SARBP_CTAS_PER_SM;
 
 
-// One pulse into the thread's MX x 2 pixels.  The two columns l = 0, 1 of a
+// One pulse into the thread's MX x 2 pixels.  The two columns l = 0, 1 (32 apart) of a
 // row form a pair and their geometry arithmetic and complex
 // multiply-accumulate run as paired FP32 instructions (__ffma2_rn and
 // friends); the sine/cosine, the shared-memory gather and the interpolation
