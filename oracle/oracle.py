@@ -28,11 +28,15 @@ _c = ctypes
 
 
 def build() -> None:
-    """Compile liboracle.so, and the reference harness when the reference
-    sources are present (make is a no-op when everything is up to date)."""
+    """Compile liboracle.so, and the reference harness when the environment
+    names a reference checkout (SARBP_REFERENCE; make is a no-op when
+    everything is up to date)."""
     import subprocess
 
-    targets = ["all"] if os.path.isdir("/root/reference/src") else [os.path.join(HERE, "liboracle.so")]
+    ref = os.environ.get("SARBP_REFERENCE", "")
+    if ref and not os.path.isdir(os.path.join(ref, "src")):
+        raise RuntimeError(f"SARBP_REFERENCE={ref} is not a reference checkout (no src/ directory)")
+    targets = ["all"] if ref else [os.path.join(HERE, "liboracle.so")]
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 
@@ -44,6 +48,7 @@ def lib():
             build()
         L = ctypes.CDLL(path)
         L.oracle_range_compress_fp64.argtypes = [_c.c_int, _c.c_int, _c.c_int, _f32p, _c.c_void_p, _f64p]
+        L.oracle_range_compress_fp64_cw.argtypes = [_c.c_int, _c.c_int, _c.c_int, _f32p, _f64p, _f64p]
         L.oracle_range_compress_ref32.argtypes = [_c.c_int, _c.c_int, _f32p, _f32p]
         bp_geo = [_f64p] * 5 + [_c.c_double] + [_c.c_int] * 3 + [_c.c_double] * 6
         L.oracle_bp_fp64.argtypes = [_c.c_int, _c.c_int, _f64p] + bp_geo + [_f64p]
@@ -57,7 +62,7 @@ def lib():
         L.oracle_dft_c128.argtypes = [_c.c_int, _f64p, _f64p, _c.c_int]
         L.oracle_mf_fp64.argtypes = ([_c.c_int, _c.c_int, _f64p] + [_f64p] * 5 + [_c.c_double] + [_c.c_int] * 3
                                      + [_c.c_double] * 6 + [_c.c_int, _f64p])
-        for f in ("oracle_range_compress_fp64", "oracle_range_compress_ref32", "oracle_bp_fp64",
+        for f in ("oracle_range_compress_fp64", "oracle_range_compress_fp64_cw", "oracle_range_compress_ref32", "oracle_bp_fp64",
                   "oracle_bp_fp64_pixels", "oracle_bp_ref32", "oracle_dft_c128", "oracle_range_compress_ref64",
                   "oracle_bp_ref64", "oracle_bp_grad_fp64", "oracle_mf_fp64"):
             getattr(L, f).restype = _c.c_int
@@ -98,11 +103,32 @@ def hamming(K: int) -> np.ndarray:
     return 0.54 - 0.46 * np.cos(2.0 * np.pi * k / (K - 1))
 
 
+def taylor(n: int, nbar: int = 5, sll: float = -35.0) -> np.ndarray:
+    """Taylor window, not normalised (the taper of matlab/rangeCompress.m:11,
+    taylorwin(K, 5, -35)): w = 1 + 2 sum_{m<nbar} F_m cos(2 pi m x),
+    x = (k - n/2 + 1/2)/n, with the coefficients F_m of Carrara, Goodman and
+    Majewski, "Spotlight Synthetic Aperture Radar" (1995)."""
+    if n <= 1:
+        return np.ones(max(n, 0))
+    A = np.arccosh(10.0 ** (-sll / 20.0)) / np.pi
+    sig2 = nbar ** 2 / (A ** 2 + (nbar - 0.5) ** 2)
+    i = np.arange(1, nbar, dtype=np.float64)
+    x = (np.arange(n, dtype=np.float64) - 0.5 * n + 0.5) / n
+    w = np.ones(n)
+    for m in range(1, nbar):
+        num = np.prod(1.0 - (m * m / sig2) / (A ** 2 + (i - 0.5) ** 2))
+        den = np.prod(1.0 - m * m / i[i != m] ** 2)
+        w += 2.0 * ((-1) ** (m + 1)) * num / (2.0 * den) * np.cos(2.0 * np.pi * m * x)
+    return w
+
+
 def window_for(name: Optional[str], K: int) -> Optional[np.ndarray]:
     if name in (None, "none"):
         return None
     if name == "hamming":
         return hamming(K)
+    if name == "taylor":
+        return taylor(K)
     raise ValueError(name)
 
 
@@ -117,6 +143,12 @@ def range_compress_fp64(ph: np.ndarray, nfft: int, window: Optional[np.ndarray] 
     ph = np.ascontiguousarray(ph, dtype=np.complex64)
     Np, K = ph.shape
     out = np.empty((Np, nfft), dtype=np.complex128)
+    if window is not None and np.iscomplexobj(window):
+        cw = np.ascontiguousarray(window, dtype=np.complex128)
+        _check(lib().oracle_range_compress_fp64_cw(K, Np, nfft, ph.view(np.float32).reshape(-1),
+                                                   cw.view(np.float64), out.view(np.float64).reshape(-1)),
+               "range_compress_fp64_cw")
+        return out
     wptr = None
     if window is not None:
         window = np.ascontiguousarray(window, dtype=np.float64)
@@ -373,3 +405,83 @@ def pga_step_reference(img: np.ndarray, db_down: float = 30.0) -> np.ndarray:
     x = np.arange(nx, dtype=np.float64)
     coeffs = np.polyfit(x, phi, 1)  # :209-212
     return phi - (coeffs[0] * x + coeffs[1])
+
+
+def ref_pga_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_pga.so"))
+
+
+def ref_pga(img: np.ndarray, iters: int) -> np.ndarray:
+    """The reference's own compiled C++ PGA, autofocus<float>()
+    (src/autofocus/cpu/autofocus_cpu.cpp:250-474, built into
+    oracle/_ref/libref_pga.so), on an image [range lines][azimuth samples];
+    returns the corrected image (complex64, same layout).  The routine prints
+    one rms line per iteration on stdout."""
+    if "pga" not in _REF:
+        L = ctypes.CDLL(os.path.join(HERE, "_ref", "libref_pga.so"))
+        L.ref_pga_f32.argtypes = [_c.c_void_p, _c.c_int, _c.c_int, _c.c_int]
+        L.ref_pga_f32.restype = _c.c_int
+        _REF["pga"] = L
+    rows, n = img.shape
+    # the routine's layout: range fastest, index r + p * numRange
+    data = np.ascontiguousarray(np.asarray(img, dtype=np.complex64).T)
+    _check(_REF["pga"].ref_pga_f32(data.ctypes.data, n, rows, int(iters)), "ref_pga_f32")
+    return np.ascontiguousarray(data.T)
+
+
+def pga_cpp_reference(img: np.ndarray, iters: int, rms_stop: float = 0.1):
+    """The reference's C++ PGA routine autofocus() (autofocus_cpu.cpp:250-474)
+    restated in double, step for step, on an image [range lines][azimuth
+    samples] (n azimuth samples).  Per iteration:
+      * each range line circularly shifted so that its largest sample (first
+        of equal maxima) lands at index n - n//2 (valarray cshift(n/2 + max),
+        :266-285);
+      * window from the non-coherent azimuth power of the UNSHIFTED image in
+        dB against its maximum (:290-305): leftIdx = the last i < n//2 below
+        -30 dB, rightIdx = the first i < n//2 with sample i + n//2 below -30 dB
+        -- the index i itself, not i + n//2, as the routine has it (:307-311)
+        -- defaults 0 and n; samples [0, leftIdx) and [rightIdx, n) zeroed;
+      * G = forward FFT of fftshift(line), fftshift = cshift((n+1)//2)
+        (:323-339, cpuBackProjection_fft.hpp:81-84);
+      * phi_dot[p+1] = sum_r Im(conj(G_p) (G_{p+1} - G_p)) / sum_r |G_p|^2,
+        phi = cumulative sum, no unwrap (:342-371);
+      * least-squares line removed (:377-402); rms = sqrt(mean(phi^2)); stop
+        before correcting when rms < 0.1 (:406-414);
+      * each range line: forward FFT, times exp(-j phi), inverse FFT with the
+        1/n scale (:418-445).
+    Returns (corrected image complex128, [phi per applied iteration], [rms])."""
+    x = np.asarray(img, dtype=np.complex128).copy()
+    rows, n = x.shape
+    h = n // 2
+    col = np.arange(n)
+    phis, rmss = [], []
+    for _ in range(int(iters)):
+        peak = np.argmax(np.abs(x), axis=1)
+        shifted = np.take_along_axis(x, (col[None, :] + h + peak[:, None]) % n, axis=1)
+        avg = np.sum((np.conj(x) * x).real, axis=0)
+        avg_db = 10.0 * np.log10(avg / avg.max())
+        left, right = -1, -1
+        for i in range(h):
+            if avg_db[i] < -30.0:
+                left = i
+            if avg_db[i + h] < -30.0 and right == -1:
+                right = i
+        left = 0 if left == -1 else left
+        right = n if right == -1 else right
+        shifted[:, :left] = 0.0
+        shifted[:, right:] = 0.0
+        G = np.fft.fft(np.roll(shifted, -((n + 1) // 2), axis=1), axis=1)
+        num = np.sum(np.imag(np.conj(G[:, :-1]) * (G[:, 1:] - G[:, :-1])), axis=0)
+        den = np.sum(np.abs(G[:, :-1]) ** 2, axis=0)
+        phi = np.cumsum(np.concatenate([[0.0], num / den]))
+        i = np.arange(n, dtype=np.float64)
+        sx, sy, sxy, sxx = i.sum(), phi.sum(), (i * phi).sum(), (i * i).sum()
+        d = n * sxx - sx * sx
+        phi = phi - ((n * sxy - sx * sy) / d * i + (sy * sxx - sx * sxy) / d)
+        rms = float(np.sqrt(np.mean(phi ** 2)))
+        rmss.append(rms)
+        if rms < rms_stop:
+            break
+        phis.append(phi)
+        x = np.fft.ifft(np.fft.fft(x, axis=1) * np.exp(-1j * phi)[None, :], axis=1)
+    return x, phis, rmss

@@ -9,8 +9,9 @@ Outputs (git-ignored, shipped with the tree):
     uncc_sar_focusing_b200/lib/libsarbp_compat.so   the reference's C++ symbols
                                                     cuda_focus_SAR_image<float,float>
                                                     and <double,double> (built only
-                                                    where the reference headers are
-                                                    present to compile against)
+                                                    when SARBP_REFERENCE names the
+                                                    reference checkout whose headers
+                                                    it compiles against)
 Register / shared-memory usage of every kernel goes to _build/ptxas.log.
 """
 from __future__ import annotations
@@ -32,7 +33,10 @@ COMPAT_LIB = os.path.join(LIBDIR, "libsarbp_compat.so")
 PROBE_LIB = os.path.join(LIBDIR, "libsarbp_probes.so")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
-REFERENCE_INCLUDE = os.environ.get("SARBP_REFERENCE_INCLUDE", "/root/reference/include")
+# the reference checkout (its headers define the shim's exported signatures);
+# the shim is built only when the environment names one
+REFERENCE = os.environ.get("SARBP_REFERENCE", "")
+REFERENCE_INCLUDE = os.path.join(REFERENCE, "include") if REFERENCE else ""
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
@@ -95,8 +99,10 @@ def build_compat(force: bool = False) -> str | None:
     SAR_Aperture / SAR_ImageFormationParameters / CArray types define the
     symbol's signature).  Skipped when they are not present."""
     src = os.path.join(CSRC, "compat", "cuda_focus_sar_image.cpp")
-    if not os.path.exists(src) or not os.path.isdir(REFERENCE_INCLUDE):
+    if not os.path.exists(src) or not REFERENCE_INCLUDE:
         return None
+    if not os.path.isdir(REFERENCE_INCLUDE):
+        raise RuntimeError(f"SARBP_REFERENCE={REFERENCE} has no include/ directory")
     if force or _newer(COMPAT_LIB, [src, LIB, os.path.join(ROOT, "include", "sarbp.h")]):
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-w", "-DCUDAFUNCTION=",
               f"-I{REFERENCE_INCLUDE}", f"-I{REFERENCE_INCLUDE}/third_party", f"-I{ROOT}/include",
