@@ -50,13 +50,33 @@ def reference_and_inputs(torch, sc):
     return desc, rc, geo, want.cpu().numpy()
 
 
-def call_noalloc(torch, desc, rc, geo, shape):
-    out = torch.full(shape, complex(7.0, -3.0), dtype=torch.complex64, device="cuda")  # stale contents
+def call_noalloc(torch, desc, rc, geo, shape, flags=0, start=None):
+    if start is None:
+        out = torch.full(shape, complex(7.0, -3.0), dtype=torch.complex64, device="cuda")  # stale contents
+    else:
+        out = torch.as_tensor(start).cuda()
     g = N.Geometry(*(ctypes.c_void_p(v.data_ptr()) for v in geo), geo[0].numel(), N.MEMORY_DEVICE)
     st = N.lib().sarbp_backproject_noalloc(ctypes.byref(desc), ctypes.c_void_p(rc.data_ptr()), ctypes.byref(g),
-                                           ctypes.c_void_p(out.data_ptr()), 0,
+                                           ctypes.c_void_p(out.data_ptr()), flags,
                                            ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
     return st, out.cpu().numpy()
+
+
+def limit_scene(num_pulses):
+    """A 64-sample, nfft-256 scene whose staged rows are 744 entries each.
+
+    The call picks 32 x 64-pixel tiles here: with lambda = nfft / max_wr =
+    16.26 bins/m and a tile half-diagonal of hypot(3.2, 6.4) m the window is
+    2 x (ceil(16.26 x 7.155) + 3) + 2 = 242 entries, the guard bands 244
+    entries each side, so a row is 256 + 2 x 244 = 744 entries.  The scratch
+    holds 2^21 - 1 entries after the error word: 2818 rows fit (2,096,592
+    entries), 2819 do not (2,097,336)."""
+    sc = S.point_target_scene(K=64, Np=num_pulses, n=40, spacing=0.2, nfft=256, snr_db=None, seed=33,
+                              n_targets=2)
+    lam = sc.nfft / sc.max_wr
+    w = int(np.ceil(lam * np.hypot(0.5 * 32 * 0.2, 0.5 * 64 * 0.2))) + 3
+    assert 2 * w + 2 == 242, "scene no longer gives the 744-entry rows this test is sized for"
+    return sc
 
 
 def test_noalloc_matches_plan_entry_point_on_two_calls_in_a_row(torch_cuda):
@@ -73,11 +93,42 @@ def test_noalloc_matches_plan_entry_point_on_two_calls_in_a_row(torch_cuda):
         assert np.isfinite(got).all()
 
 
+def test_noalloc_runs_on_the_device_its_descriptor_names(torch_cuda):
+    torch = torch_cuda
+    sc = S.point_target_scene(K=64, Np=40, n=40, spacing=0.2, nfft=256, snr_db=None, seed=35, n_targets=3)
+    desc, rc, geo, want = reference_and_inputs(torch, sc)
+    desc.device = torch.cuda.current_device()
+    st, got = call_noalloc(torch, desc, rc, geo, want.shape)
+    assert st == N.SARBP_OK, N.lib().sarbp_status_string(st)
+    assert O.rel_l2(got, want) < MIXED_TOL
+    desc.device = torch.cuda.device_count()  # no such device
+    st, _ = call_noalloc(torch, desc, rc, geo, want.shape)
+    assert st == N.SARBP_ERR_INVALID_ARGUMENT
+
+
+def test_noalloc_accumulates_into_the_callers_image(torch_cuda):
+    torch = torch_cuda
+    sc = S.point_target_scene(K=64, Np=40, n=40, spacing=0.2, nfft=256, snr_db=None, seed=34, n_targets=3)
+    desc, rc, geo, want = reference_and_inputs(torch, sc)
+    rng = np.random.default_rng(5)
+    start = (rng.standard_normal(want.shape) + 1j * rng.standard_normal(want.shape)).astype(np.complex64)
+    start *= np.float32(np.abs(want).max())
+    st, got = call_noalloc(torch, desc, rc, geo, want.shape, flags=N.ACCUMULATE, start=start)
+    assert st == N.SARBP_OK, N.lib().sarbp_status_string(st)
+    assert O.rel_l2(got - start, want) < MIXED_TOL
+
+
+def test_noalloc_serves_the_largest_request_its_scratch_holds(torch_cuda):
+    torch = torch_cuda
+    desc, rc, geo, want = reference_and_inputs(torch, limit_scene(2818))
+    st, got = call_noalloc(torch, desc, rc, geo, want.shape)
+    assert st == N.SARBP_OK, N.lib().sarbp_status_string(st)
+    assert O.rel_l2(got, want) < MIXED_TOL
+
+
 def test_noalloc_rejects_requests_beyond_its_scratch(torch_cuda):
     torch = torch_cuda
-    sc = S.point_target_scene(K=64, Np=40, n=40, spacing=0.2, nfft=256, snr_db=None, seed=33, n_targets=2)
+    sc = limit_scene(2819)
     desc, rc, geo, want = reference_and_inputs(torch, sc)
-    desc.nfft = 1 << 22  # 40 pulses x 4M bins x 16 B is far beyond 32 MiB
-    big_rc = torch.zeros(1, dtype=torch.complex64, device="cuda")
-    st, _ = call_noalloc(torch, desc, big_rc, geo, want.shape)
+    st, _ = call_noalloc(torch, desc, rc, geo, want.shape)
     assert st == N.SARBP_ERR_UNSUPPORTED

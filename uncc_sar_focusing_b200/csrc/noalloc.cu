@@ -27,6 +27,7 @@
 #include <mutex>
 
 #include "bp_common.cuh"
+#include "host_common.h"
 #include "sarbp_internal.h"
 
 namespace {
@@ -137,10 +138,27 @@ extern "C" SARBP_API int sarbp_backproject_noalloc(const sarbp_plan_desc *desc, 
     const long long total = row_stride * geo->num_pulses;
     if (total > static_cast<long long>(kScratchEntries) - 1) return SARBP_ERR_UNSUPPORTED;  // beyond 32 MiB
 
+    // desc->device >= 0: run on that device (as sarbp_plan_create does), the
+    // caller's current device restored on return; -1: the current device
+    if (desc->device < -1) return SARBP_ERR_INVALID_ARGUMENT;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
         return SARBP_ERR_NO_DEVICE;
+    }
+    if (desc->device >= 0) {
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess) {
+            cudaGetLastError();
+            return SARBP_ERR_NO_DEVICE;
+        }
+        if (desc->device >= count) return SARBP_ERR_INVALID_ARGUMENT;
+        dev = desc->device;
+    }
+    host::DeviceGuard on_device(dev);
+    if (on_device.status != cudaSuccess) {
+        cudaGetLastError();
+        return SARBP_ERR_CUDA;
     }
     float4 *scratch = nullptr;
     int st = scratch_for(dev, &scratch);
@@ -190,9 +208,11 @@ extern "C" SARBP_API int sarbp_backproject_noalloc(const sarbp_plan_desc *desc, 
         L.nhyp = 1;
         e = launch_bp_mixed(L, tc, false, smem, s);
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    // the error word comes back on the call's own stream, behind its kernels:
+    // one stream synchronisation, nothing ordered against other streams
     unsigned bits = 0;
-    if (e == cudaSuccess) e = cudaMemcpy(&bits, err, sizeof(bits), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bits, err, sizeof(bits), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return SARBP_ERR_CUDA;
