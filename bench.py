@@ -104,6 +104,15 @@ def make_scene(config: str, rank: int, world: int, device):
     return sc, desc
 
 
+def config_dict(sc, desc: str, world: int) -> dict:
+    """The workload as both arms report it (identical dicts for the same
+    --config and world size)."""
+    return {"workload": desc, "pixels_per_gpu": sc.grid.npix, "pulses": sc.num_pulses,
+            "range_samples": sc.num_range_samples, "nfft": sc.nfft, "pixel_pulses_per_step_per_gpu": sc.pixel_pulses,
+            "l2": "inputs larger than L2 (range-profile pair rows of every pulse, 16 B per entry)",
+            "parallelism": f"{world} image slab(s), one per GPU, no data-path collective"}
+
+
 # ---------------------------------------------------------------------------
 # clocks during the timed region
 # ---------------------------------------------------------------------------
@@ -255,10 +264,12 @@ def reference_arm(args):
         if i >= args.warmup:
             vals.append(info["value"])
     value = statistics.median(vals)
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": info["seconds"] * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": desc, "precision": "reference float (run_bp<float>)"},
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (the reference's run_bp<float>)", "data": "synthetic",
+            "config": config_dict(sc, desc, world),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
                              "sample": info["sample"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -310,9 +321,12 @@ def autofocus_section(dev, grid_seconds: float):
     track error up to 1.5 m plus a 1 mm/pulse random walk): the gradient
     pipeline (cubic coefficients, then per-pulse line of sight, then PGA)
     against the reference's multiresolution grid search restated on the same
-    engine (6 quadratic/cubic coefficients, 5 points each, halving boxes),
-    bounded to grid_seconds.  Seconds-to-focus = time for each method to reach
-    the grid search's final entropy."""
+    engine (the reference's searched coefficients -- slope and quadratic term
+    per axis -- 5 points each, halving boxes, every grid point scored with the
+    reference's own 2-D DFT cost), bounded to grid_seconds.  Both final images
+    carry the Shannon entropy and the reference's two costs (DFT and column
+    histogram).  Seconds-to-focus = time for each method to reach the grid
+    search's final Shannon entropy."""
     import numpy as np
     import torch
 
@@ -334,8 +348,12 @@ def autofocus_section(dev, grid_seconds: float):
         grad = AF.focus_motion_error(plan, ax, ay, az, r0, f0)
         motion = AF.CubicMotion(ax, ay, az)
         grid = AF.grid_search_autofocus(plan, motion, r0, f0, span=1.5, points=5, levels=4, batch=128,
-                                        deadline_s=grid_seconds)
-    e_grid = grid.history[-1]["entropy"] if grid.history else float("nan")
+                                        deadline_s=grid_seconds, cost="reference_dft")
+        a = motion.track(grid.theta)
+        img_grid = plan.backproject(a[0].contiguous(), a[1].contiguous(), a[2].contiguous(), r0, f0)
+        metrics_grid = AF.focus_metrics(img_grid)
+        metrics_grad = AF.focus_metrics(grad["image"])
+    e_grid = metrics_grid["shannon_entropy"]
     t_grad = AF.time_to_entropy(grad["timeline"], e_grid)
     return {
         "workload": "autofocus: 9.6 GHz / 600 MHz, 4 deg at 10 km, 30 deg el, 1024 pulses x 512 samples, 512^2 "
@@ -344,10 +362,16 @@ def autofocus_section(dev, grid_seconds: float):
         "entropy_measured_track": e_measured, "entropy_true_track": e_true,
         "gradient": {"entropy_cubic": grad["entropy_cubic"], "entropy_line_of_sight": grad["entropy_los"],
                      "entropy_pga": grad["entropy_pga"], "seconds": grad["seconds"],
+                     "final_image": metrics_grad,
                      "stages": "Adam on 12 cubic coefficients (300 it) -> Adam on 1024 per-pulse ranges "
-                               "(200 it) -> PGA; gradients from the adjoint kernel"},
-        "grid_search": {"entropy": e_grid, "seconds": grid.seconds, "images": grid.images_formed,
-                        "levels_done": len(grid.history), "bounded_to_s": grid_seconds},
+                               "(200 it) -> PGA (PGA.m semantics, on the device); gradients from the adjoint "
+                               "kernel"},
+        "grid_search": {"cost": "reference_dft", "entropy": e_grid, "seconds": grid.seconds,
+                        "images": grid.images_formed, "levels_done": len(grid.history),
+                        "bounded_to_s": grid_seconds, "final_image": metrics_grid,
+                        "searched": "slope and quadratic term of each axis (the reference's quadratic search "
+                                    "without its velocity scale), 5 points each, box halved per level; the 12 "
+                                    "cubic coefficients at 5 points would be 5^12 images per level"},
         "sec_to_focus": {"target_entropy": e_grid, "gradient_s": t_grad, "grid_search_s": grid.seconds,
                          "speedup": (grid.seconds / t_grad) if t_grad else None},
     }
@@ -713,20 +737,24 @@ def gpu_arm(args):
         # rows the backprojection reads out: 8 B per sample + 16 B per entry
         # (nfft + 1 entries per pulse)
         rc_bytes = sc.num_pulses * (sc.num_range_samples * 8 + (sc.nfft + 1) * 16)
+        mixed_speedup = fp64_ms / bp_ms
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32+f64 (FP64 per-tile geometry, FP32 per pixel-pulse)",
+            "vs_baseline": None,
+            # the north-star ratio first, so that a truncated record keeps it:
+            # backprojection kernel, mixed precision against all-FP64, same
+            # inputs and GPU, and the mixed image's error against the FP64 one
+            "mixed_vs_fp64_gpu": {"bp_speedup": mixed_speedup, "rel_l2": rel, "peak_phase_error_rad": phase_err,
+                                  "tolerance": 1e-4, "mixed_bp_ms": bp_ms, "fp64_bp_ms": fp64_ms},
+            "dtype": "f32+f64 (FP64 per-tile geometry, FP32 per pixel-pulse)",
             "data": "synthetic",
-            "config": {"workload": desc, "pixels_per_gpu": sc.grid.npix, "pulses": sc.num_pulses,
-                       "range_samples": sc.num_range_samples, "nfft": sc.nfft, "precision": "mixed",
-                       "pixel_pulses_per_step_per_gpu": pp,
-                       "l2": "inputs larger than L2 (range-profile pair buffer "
-                             f"{plan.workspace_bytes / 2**20:.0f} MiB plan workspace)",
-                       "parallelism": f"{world} image slab(s), one per GPU, no data-path collective"},
-            "accuracy": {"rel_l2_mixed_vs_fp64_gpu": rel, "peak_phase_error_rad": phase_err, "tolerance": 1e-4},
-            "fp64_gpu": {"bp_value": pp / (fp64_ms * 1e-3), "unit": UNIT,
-                         "mixed_speedup": (pp / (bp_ms * 1e-3)) / (pp / (fp64_ms * 1e-3))},
+            "config": config_dict(sc, desc, world),
+            "plan_workspace_mib": plan.workspace_bytes / 2**20,
+            "accuracy": {"rel_l2_mixed_vs_fp64_gpu": rel, "peak_phase_error_rad": phase_err, "tolerance": 1e-4,
+                         "note": "against the FP64 GPU path on the full image; that path is checked against "
+                                 "the FP64 CPU oracle on small scenes (1e-13) and on sampled pixels of this one"},
+            "fp64_gpu": {"bp_value": pp / (fp64_ms * 1e-3), "unit": UNIT, "mixed_speedup": mixed_speedup},
             "e2e": {"value": world * pp / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3,
                     "api": "sarbp_focus_submit/sarbp_focus_wait, pinned host buffers",
@@ -758,7 +786,11 @@ def gpu_arm(args):
         if world == 1 and not args.no_batched:
             line["batched"] = batched_section(dev, args.steps)
         if world == 1 and not args.no_volumetric:
-            line["volumetric"] = volumetric_section(dev, args.steps)
+            vol = volumetric_section(dev, args.steps)
+            line["volumetric"] = vol
+            if "fp64" in vol:
+                line["mixed_vs_fp64_gpu"]["volumetric_bp_speedup"] = vol["fp64"]["mixed_speedup"]
+                line["mixed_vs_fp64_gpu"]["volumetric_rel_l2"] = vol["rel_l2_vs_fp64"]["total"]
         traffic = profiled_traffic(args.config)
         if traffic is not None:
             line["roofline"]["traffic"] = traffic
