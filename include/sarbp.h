@@ -85,7 +85,9 @@ enum {
 /* Range taper applied before zero padding */
 enum {
     SARBP_WINDOW_NONE = 0,
-    SARBP_WINDOW_HAMMING = 1 /* 0.54 - 0.46 cos(2 pi k / (K-1)) */
+    SARBP_WINDOW_HAMMING = 1, /* 0.54 - 0.46 cos(2 pi k / (K-1)) (matlab/formImage3DSAR.m:115-116) */
+    SARBP_WINDOW_TAYLOR = 2   /* Taylor window, 5 nearly constant sidelobes at -35 dB: the range
+                                 factor of taylorwin(K, 5, -35) in matlab/rangeCompress.m:11 */
 };
 
 /* Where a pointer lives */
@@ -177,6 +179,18 @@ SARBP_API int sarbp_plan_get_info(const sarbp_plan *plan, sarbp_plan_info *info)
  * kept inside the plan for the next sarbp_backproject. */
 SARBP_API int sarbp_range_compress(sarbp_plan *plan, const void *phase_history, int num_pulses, int memory,
                          void *stream);
+
+/* Caller-supplied range weights in place of the plan's taper: complex128
+ * [num_range_samples] (interleaved re, im doubles, HOST memory), multiplied
+ * into every pulse's samples before the zero pad and inverse FFT -- a
+ * taper, a reference function for matched filtering in range, or both
+ * (matlab/rangeCompress.m:6-7 takes a caller's taper_window the same way,
+ * for the range axis).  NULL restores the plan's desc.window.  The weights
+ * fold into the per-sample factor the range-compression kernels already
+ * apply (no extra work per sample); sarbp_matched_filter uses them too.
+ * Waits for the plan's outstanding submissions; work the caller queued with
+ * this plan on its own streams must be complete. */
+SARBP_API int sarbp_plan_set_range_weights(sarbp_plan *plan, const double *weights);
 
 /* Copy the plan's range profiles out: complex64 (MIXED) or complex128 (FP64)
  * [num_pulses][nfft]. */
@@ -313,7 +327,9 @@ SARBP_API int sarbp_plan_check(sarbp_plan *plan, void *stream);
  * Inputs and output are device memory the caller owns: range profiles
  * complex64 [num_pulses][nfft] (as sarbp_get_range_profiles returns them),
  * geometry (memory must be SARBP_MEMORY_DEVICE), image complex64 on desc's
- * grid.  desc supplies nfft, max_wr and the grid; precision must be
+ * grid.  desc supplies nfft, max_wr, the grid and the device (>= 0: the
+ * call runs on that device and restores the caller's current device before
+ * returning; -1: the current device); precision must be
  * SARBP_PRECISION_MIXED; flags may be SARBP_ACCUMULATE.  Allocates nothing:
  * its scratch is a fixed 32 MiB file-scope device array per GPU, held until
  * the process exits; requests whose staged rows, num_pulses x (nfft + 2 x

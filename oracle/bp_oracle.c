@@ -49,7 +49,25 @@
  * ifft includes the 1/nfft scale; fftshift moves element (i + (nfft+1)/2) % nfft
  * to position i.
  */
+static int range_compress_fp64_impl(int K, int Np, int nfft, const float *ph, const double *window,
+                                    const double *cweights, double *rc);
+
 int oracle_range_compress_fp64(int K, int Np, int nfft, const float *ph, const double *window, double *rc) {
+    return range_compress_fp64_impl(K, Np, nfft, ph, window, NULL, rc);
+}
+
+/*
+ * The same with complex per-sample weights c_k (interleaved doubles [K]) in
+ * place of the real taper: rc_p = fftshift(ifft(c .* ph_p, nfft)), the
+ * caller-supplied range weights of sarbp_plan_set_range_weights (a taper, a
+ * range reference function, or both; matlab/rangeCompress.m:6-7).
+ */
+int oracle_range_compress_fp64_cw(int K, int Np, int nfft, const float *ph, const double *cweights, double *rc) {
+    return range_compress_fp64_impl(K, Np, nfft, ph, NULL, cweights, rc);
+}
+
+static int range_compress_fp64_impl(int K, int Np, int nfft, const float *ph, const double *window,
+                                    const double *cweights, double *rc) {
     if (K <= 0 || Np <= 0 || nfft < K || !ph || !rc) return -1;
     const int shift = (nfft + 1) / 2;
     int err = 0;
@@ -63,9 +81,16 @@ int oracle_range_compress_fp64(int K, int Np, int nfft, const float *ph, const d
             for (int k = 0; k < nfft; k++) {
                 double re = 0.0, im = 0.0;
                 if (k < K) {
-                    const double w = window ? window[k] : 1.0;
-                    re = w * (double)ph[2 * ((size_t)p * K + k)];
-                    im = w * (double)ph[2 * ((size_t)p * K + k) + 1];
+                    const double vr = (double)ph[2 * ((size_t)p * K + k)];
+                    const double vi = (double)ph[2 * ((size_t)p * K + k) + 1];
+                    if (cweights) {
+                        re = cweights[2 * k] * vr - cweights[2 * k + 1] * vi;
+                        im = cweights[2 * k] * vi + cweights[2 * k + 1] * vr;
+                    } else {
+                        const double w = window ? window[k] : 1.0;
+                        re = w * vr;
+                        im = w * vi;
+                    }
                 }
                 buf[2 * k] = re;
                 buf[2 * k + 1] = im;

@@ -189,3 +189,26 @@ def test_mf_oracle_pinned_to_reference_run_mf():
 def test_mf_is_nfft_times_bp_up_to_interpolation():
     sc = _mf_scene(K=64, Np=48, n=32, spacing=0.15, nfft=512, snr_db=20.0, seed=3, n_targets=4, extent=4.0)
     assert O.rel_l2(O.focus_fp64(sc) * sc.nfft, O.mf_fp64(sc)) < 0.03
+
+
+def test_taylor_window_matches_scipy():
+    """The oracle's Taylor taper (matlab/rangeCompress.m:11, taylorwin(K, 5,
+    -35), not normalised) against scipy's independent implementation."""
+    from scipy.signal import windows
+
+    for n in (1, 2, 7, 64, 424, 512, 1001):
+        want = windows.taylor(n, nbar=5, sll=35, norm=False)
+        assert np.allclose(O.taylor(n), want, rtol=0, atol=1e-12), n
+
+
+def test_complex_range_weights_oracle_is_the_weighted_transform():
+    """Range compression with complex per-sample weights equals the plain
+    oracle transform of the weighted phase history (numpy FFT in FP64)."""
+    rng = np.random.default_rng(3)
+    ph = (rng.standard_normal((5, 48)) + 1j * rng.standard_normal((5, 48))).astype(np.complex64)
+    w = rng.standard_normal(48) + 1j * rng.standard_normal(48)
+    got = O.range_compress_fp64(ph, 200, w)
+    x = np.zeros((5, 200), dtype=np.complex128)
+    x[:, :48] = ph.astype(np.complex128) * w[None, :]
+    want = np.fft.fftshift(np.fft.ifft(x, axis=1), axes=1)
+    assert np.abs(got - want).max() < 1e-13 * np.abs(want).max() * 200

@@ -29,6 +29,7 @@ PRECISION_MIXED = 0
 PRECISION_FP64 = 1
 WINDOW_NONE = 0
 WINDOW_HAMMING = 1
+WINDOW_TAYLOR = 2
 MEMORY_HOST = 0
 MEMORY_DEVICE = 1
 ACCUMULATE = 1
@@ -41,7 +42,7 @@ EXPORTED = (
     "sarbp_focus", "sarbp_focus_image", "sarbp_plan_check", "sarbp_backproject_noalloc",
     "sarbp_backproject_adjoint", "sarbp_backproject_hypotheses", "sarbp_focus_submit", "sarbp_focus_wait", "sarbp_plan_get_info",
     "sarbp_batch_create", "sarbp_batch_destroy", "sarbp_batch_focus", "sarbp_batch_wait", "sarbp_batch_autotune",
-    "sarbp_batch_get_info", "sarbp_batch_set_schedule", "sarbp_matched_filter",
+    "sarbp_batch_get_info", "sarbp_batch_set_schedule", "sarbp_matched_filter", "sarbp_plan_set_range_weights",
 )
 
 
@@ -121,6 +122,7 @@ def lib():
         L.sarbp_batch_get_info.argtypes = [vp, P(BatchInfo)]
         L.sarbp_batch_set_schedule.argtypes = [vp, i]
         L.sarbp_matched_filter.argtypes = [vp, P(Aperture), vp, i, vp]
+        L.sarbp_plan_set_range_weights.argtypes = [vp, vp]
         for name in EXPORTED:
             if name != "sarbp_status_string":
                 getattr(L, name).restype = i

@@ -147,6 +147,19 @@ int alloc(sarbp_plan *p, void **ptr, size_t bytes) {
 
 size_t cplx_bytes(const sarbp_plan *p) { return p->precision == SARBP_PRECISION_FP64 ? 16 : 8; }
 
+// The per-sample factor table of the range-compression kernels from the
+// plan's weights (the caller's, else the desc's taper).
+int upload_range_factors(sarbp_plan *p) {
+    const std::vector<double> fac = range_factors(p->desc, p->range_w.empty() ? nullptr : p->range_w.data());
+    if (p->precision == SARBP_PRECISION_FP64) {
+        SARBP_TRY_CUDA(cudaMemcpy(p->d_fac, fac.data(), fac.size() * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> f32(fac.begin(), fac.end());
+        SARBP_TRY_CUDA(cudaMemcpy(p->d_fac, f32.data(), f32.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    return SARBP_OK;
+}
+
 int check_geometry_host(const sarbp_geometry *g) {
     const double *arrs[5] = {g->ant_x, g->ant_y, g->ant_z, g->slant_range, g->start_freq};
     for (const double *a : arrs)
@@ -545,12 +558,12 @@ int matched_filter_impl(sarbp_plan *p, const sarbp_aperture *ap, void *image, in
         (geo->memory != SARBP_MEMORY_HOST && geo->memory != SARBP_MEMORY_DEVICE) ||
         (image_memory != SARBP_MEMORY_HOST && image_memory != SARBP_MEMORY_DEVICE))
         return SARBP_ERR_INVALID_ARGUMENT;
-    if (p->desc.window == SARBP_WINDOW_HAMMING && !p->d_win) {
-        std::vector<double> w(static_cast<size_t>(p->K), 1.0);
-        for (int k = 0; k < p->K && p->K > 1; ++k)
-            w[k] = 0.54 - 0.46 * std::cos(2.0 * M_PI * static_cast<double>(k) / static_cast<double>(p->K - 1));
-        SARBP_TRY(alloc(p, reinterpret_cast<void **>(&p->d_win), w.size() * sizeof(double)));
+    const bool weighted = p->desc.window != SARBP_WINDOW_NONE || !p->range_w.empty();
+    if (weighted && (!p->d_win || p->win_stale)) {
+        const std::vector<double> w = range_weights(p->desc, p->range_w.empty() ? nullptr : p->range_w.data());
+        if (!p->d_win) SARBP_TRY(alloc(p, reinterpret_cast<void **>(&p->d_win), w.size() * sizeof(double)));
         SARBP_TRY_CUDA(cudaMemcpy(p->d_win, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice));
+        p->win_stale = false;
     }
     const void *ph = ap->phase_history;
     if (ap->phase_history_memory == SARBP_MEMORY_HOST) {
@@ -581,8 +594,7 @@ int matched_filter_impl(sarbp_plan *p, const sarbp_aperture *ap, void *image, in
     M.dy = p->dy;
     M.dz = p->dz;
     M.img = dimg;
-    SARBP_TRY_CUDA(launch_mf(ph, p->desc.window == SARBP_WINDOW_HAMMING ? p->d_win : nullptr, M,
-                             p->precision == SARBP_PRECISION_FP64, s));
+    SARBP_TRY_CUDA(launch_mf(ph, weighted ? p->d_win : nullptr, M, p->precision == SARBP_PRECISION_FP64, s));
     if (image_memory == SARBP_MEMORY_HOST) {
         SARBP_TRY_CUDA(cudaMemcpyAsync(image, dimg, img_bytes, cudaMemcpyDeviceToHost, s));
         return read_errors(p, s);
@@ -690,20 +702,10 @@ int sarbp_plan_create(const sarbp_plan_desc *desc, sarbp_plan **out) {
         return SARBP_ERR_CUDA;
     }
     // fac[k] = w_k / nfft * exp(+j 2 pi ((k s) mod nfft) / nfft), s = (nfft+1)/2
-    {
-        const std::vector<double> fac = range_factors(*desc);
-        cudaError_t e;
-        if (p->precision == SARBP_PRECISION_FP64) {
-            e = cudaMemcpy(p->d_fac, fac.data(), fac.size() * sizeof(double), cudaMemcpyHostToDevice);
-        } else {
-            std::vector<float> f32(fac.begin(), fac.end());
-            e = cudaMemcpy(p->d_fac, f32.data(), f32.size() * sizeof(float), cudaMemcpyHostToDevice);
-        }
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            release(p);
-            return from_cuda(e);
-        }
+    st = upload_range_factors(p);
+    if (st != SARBP_OK) {
+        release(p);
+        return st;
     }
     // fused range compression when the shape has a kernel (environment
     // SARBP_RC=cufft keeps the taper / cuFFT / pair-row path)
@@ -773,6 +775,24 @@ int sarbp_plan_get_info(const sarbp_plan *plan, sarbp_plan_info *info) {
     info->kernels_per_backproject = (plan->d_sk && plan->sk_resident > 0 && info->tiles % plan->sk_resident != 0) ? 2 : 1;
     info->fused_range_compression = plan->d_rctab ? 1 : 0;
     return SARBP_OK;
+}
+
+int sarbp_plan_set_range_weights(sarbp_plan *plan, const double *weights) {
+    if (!plan) return SARBP_ERR_NULL_POINTER;
+    if (weights)
+        for (int k = 0; k < 2 * plan->K; ++k)
+            if (!std::isfinite(weights[k])) return SARBP_ERR_INVALID_ARGUMENT;
+    DeviceGuard guard(plan->device);
+    SARBP_TRY_CUDA(guard.status);
+    SARBP_TRY(drain_pipe(plan));
+    // the kernels of earlier calls on any stream may still read the table
+    SARBP_TRY_CUDA(cudaDeviceSynchronize());
+    if (weights)
+        plan->range_w.assign(weights, weights + 2 * static_cast<size_t>(plan->K));
+    else
+        plan->range_w.clear();
+    plan->win_stale = true;
+    return upload_range_factors(plan);
 }
 
 int sarbp_range_compress(sarbp_plan *plan, const void *phase_history, int num_pulses, int memory, void *stream) {

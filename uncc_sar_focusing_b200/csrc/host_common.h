@@ -76,7 +76,8 @@ inline int validate_desc(const sarbp_plan_desc *d) {
         return SARBP_ERR_INVALID_ARGUMENT;
     if (d->precision != SARBP_PRECISION_MIXED && d->precision != SARBP_PRECISION_FP64)
         return SARBP_ERR_INVALID_ARGUMENT;
-    if (d->window != SARBP_WINDOW_NONE && d->window != SARBP_WINDOW_HAMMING) return SARBP_ERR_INVALID_ARGUMENT;
+    if (d->window != SARBP_WINDOW_NONE && d->window != SARBP_WINDOW_HAMMING && d->window != SARBP_WINDOW_TAYLOR)
+        return SARBP_ERR_INVALID_ARGUMENT;
     const double samples = static_cast<double>(d->num_pulses) * static_cast<double>(d->nfft);
     if (samples > 4.0e9) return SARBP_ERR_UNSUPPORTED;
     return SARBP_OK;
@@ -116,18 +117,70 @@ inline void near_field_consts(double hd, double *near_hd16, double *near_coef) {
 // fac[k] = w_k / nfft * exp(+j 2 pi ((k s) mod nfft) / nfft), s = (nfft+1)/2,
 // interleaved re, im: taper (Hamming or none), the 1/nfft of the inverse FFT
 // and the fftshift as an input twiddle.
-inline std::vector<double> range_factors(const sarbp_plan_desc &d) {
+// Taylor window of n samples with nbar nearly constant sidelobes at sll dB
+// (sll < 0), not normalised: w_k = 1 + 2 sum_{m=1}^{nbar-1} F_m cos(2 pi m x_k),
+// x_k = (k - n/2 + 1/2) / n, with the coefficients of Carrara, Goodman and
+// Majewski, "Spotlight Synthetic Aperture Radar" (1995), sec. on Taylor
+// weighting: A = acosh(10^(-sll/20)) / pi, sigma^2 = nbar^2 / (A^2 + (nbar -
+// 1/2)^2), F_m = (-1)^(m+1) prod_i (1 - m^2 / (sigma^2 (A^2 + (i - 1/2)^2)))
+// / (2 prod_{i != m} (1 - m^2 / i^2)), i = 1 .. nbar-1.  This is the taper
+// matlab/rangeCompress.m:11 applies as taylorwin(K, 5, -35).
+inline std::vector<double> taylor_window(int n, int nbar, double sll) {
+    std::vector<double> w(static_cast<size_t>(n > 0 ? n : 0), 1.0);
+    if (n <= 1) return w;  // a single sample keeps unit weight
+    const double A = std::acosh(std::pow(10.0, -sll / 20.0)) / M_PI;
+    const double sig2 = nbar * nbar / (A * A + (nbar - 0.5) * (nbar - 0.5));
+    for (int m = 1; m < nbar; ++m) {
+        double num = 1.0, den = 1.0;
+        for (int i = 1; i < nbar; ++i) {
+            num *= 1.0 - (static_cast<double>(m) * m / sig2) / (A * A + (i - 0.5) * (i - 0.5));
+            if (i != m) den *= 1.0 - static_cast<double>(m) * m / (static_cast<double>(i) * i);
+        }
+        const double Fm = ((m % 2) ? 1.0 : -1.0) * num / (2.0 * den);
+        for (int k = 0; k < n; ++k) {
+            const double x = (k - 0.5 * n + 0.5) / n;
+            w[k] += 2.0 * Fm * std::cos(2.0 * M_PI * m * x);
+        }
+    }
+    return w;
+}
+
+// Real taper w_k of a plan's window (all ones for SARBP_WINDOW_NONE).
+inline std::vector<double> taper(int K, int window) {
+    if (window == SARBP_WINDOW_TAYLOR) return taylor_window(K, 5, -35.0);
+    std::vector<double> w(static_cast<size_t>(K), 1.0);
+    if (window == SARBP_WINDOW_HAMMING && K > 1)
+        for (int k = 0; k < K; ++k)
+            w[k] = 0.54 - 0.46 * std::cos(2.0 * M_PI * static_cast<double>(k) / static_cast<double>(K - 1));
+    return w;
+}
+
+// Per-sample complex weights c_k (interleaved): the caller's, else the taper.
+inline std::vector<double> range_weights(const sarbp_plan_desc &d, const double *user) {
+    const int K = d.num_range_samples;
+    std::vector<double> c(2 * static_cast<size_t>(K), 0.0);
+    if (user) {
+        c.assign(user, user + 2 * static_cast<size_t>(K));
+        return c;
+    }
+    const std::vector<double> w = taper(K, d.window);
+    for (int k = 0; k < K; ++k) c[2 * k] = w[k];
+    return c;
+}
+
+// fac[k] = c_k / nfft * exp(+j 2 pi ((k s) mod nfft) / nfft), s = (nfft+1)/2:
+// weight, 1/nfft scale and the fftshift moved to the input side as a twiddle.
+inline std::vector<double> range_factors(const sarbp_plan_desc &d, const double *user = nullptr) {
     const int K = d.num_range_samples, N = d.nfft;
     const long long s = (N + 1) / 2;
+    const std::vector<double> c = range_weights(d, user);
     std::vector<double> fac(2 * static_cast<size_t>(K));
     for (int k = 0; k < K; ++k) {
-        double w = 1.0;
-        if (d.window == SARBP_WINDOW_HAMMING && K > 1)
-            w = 0.54 - 0.46 * std::cos(2.0 * M_PI * static_cast<double>(k) / static_cast<double>(K - 1));
         const long long m = (static_cast<long long>(k) * s) % N;
         const double ang = 2.0 * M_PI * static_cast<double>(m) / static_cast<double>(N);
-        fac[2 * k] = w / N * std::cos(ang);
-        fac[2 * k + 1] = w / N * std::sin(ang);
+        const double tr = std::cos(ang) / N, ti = std::sin(ang) / N;
+        fac[2 * k] = c[2 * k] * tr - c[2 * k + 1] * ti;
+        fac[2 * k + 1] = c[2 * k] * ti + c[2 * k + 1] * tr;
     }
     return fac;
 }

@@ -60,9 +60,9 @@ __global__ void __launch_bounds__(kMfThreads) mf_kernel(const float2 *__restrict
             __syncthreads();
             for (int k = c0 + threadIdx.x; k < c1; k += kMfThreads) {
                 const float2 v = ph[static_cast<long long>(p) * M.K + k];
-                const double w = win ? win[k] : 1.0;
-                s[k - c0].x = static_cast<R>(w * v.x);
-                s[k - c0].y = static_cast<R>(w * v.y);
+                const double wr = win ? win[2 * k] : 1.0, wi = win ? win[2 * k + 1] : 0.0;
+                s[k - c0].x = static_cast<R>(wr * v.x - wi * v.y);
+                s[k - c0].y = static_cast<R>(wr * v.y + wi * v.x);
             }
             __syncthreads();
             for (int k = c1 - 1; k >= c0; --k) {

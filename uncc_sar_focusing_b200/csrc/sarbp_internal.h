@@ -64,6 +64,7 @@ struct MfLaunch {
     double left, bottom, zlow, dx, dy, dz;
     void *img;
 };
+// win: complex range weights (interleaved double re, im) [K], or null (all ones)
 cudaError_t launch_mf(const void *ph, const double *win, const MfLaunch &M, bool fp64, cudaStream_t s);
 
 // Tile shape of the forward kernels (see bp_mixed.cu).
@@ -156,7 +157,9 @@ struct sarbp_plan {
     double *d_gout;   // adjoint output staging for host outputs [4][np] (allocated on first use)
     void *d_hyp;      // host-memory staging for hypothesis batches (allocated on first use)
     size_t hyp_bytes;
-    double *d_win;    // taper w_k for the matched filter (allocated on first use)
+    double *d_win;    // complex range weights c_k for the matched filter (allocated on first use)
+    bool win_stale;   // d_win no longer holds the current weights
+    std::vector<double> range_w;  // caller's complex range weights [2 K] (empty: desc.window)
     void *d_rctab;    // twiddle table of the fused range compression (null: cuFFT path)
     int rc_R;         // nfft / K of the fused range compression
     int rc_grid;      // its CTAs

@@ -18,7 +18,7 @@ from . import _native as N
 from .scenes import CLIGHT, Grid, Scene
 
 _PRECISION = {"mixed": N.PRECISION_MIXED, "fp64": N.PRECISION_FP64}
-_WINDOW = {None: N.WINDOW_NONE, "none": N.WINDOW_NONE, "hamming": N.WINDOW_HAMMING}
+_WINDOW = {None: N.WINDOW_NONE, "none": N.WINDOW_NONE, "hamming": N.WINDOW_HAMMING, "taylor": N.WINDOW_TAYLOR}
 
 
 def _is_torch(x) -> bool:
@@ -127,6 +127,19 @@ class Plan:
         return torch.zeros(self.image_shape(), dtype=dt, device=device)
 
     # -- entry points -------------------------------------------------------
+    def set_range_weights(self, weights) -> None:
+        """Complex per-sample range weights (a taper, a range reference
+        function, or both; length K) in place of the plan's window; None
+        restores the window (sarbp_plan_set_range_weights)."""
+        if weights is None:
+            N.check(N.lib().sarbp_plan_set_range_weights(self._h, None), "sarbp_plan_set_range_weights")
+            return
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.complex128).reshape(-1))
+        if w.shape[0] != self.K:
+            raise ValueError(f"range weights need {self.K} values, got {w.shape[0]}")
+        N.check(N.lib().sarbp_plan_set_range_weights(self._h, ctypes.c_void_p(w.ctypes.data)),
+                "sarbp_plan_set_range_weights")
+
     def range_compress(self, phase_history) -> None:
         n = int(phase_history.shape[0])
         p, mem, keep = _ptr(phase_history, np.complex64, n * self.K)
