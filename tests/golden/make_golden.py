@@ -5,8 +5,13 @@ and <double,double>, src/cpuBackProjection/cpuBackProjection.hpp:95-163,230-262)
 compiled from its own sources by oracle/Makefile into oracle/_ref/, on small
 seeded point-target scenes, and stores inputs and outputs as .npz.  The GPU box
 has no reference sources, so these files are how the oracle stays pinned there.
+With --pga it writes the PGA fixtures instead: the reference's C++ PGA routine
+(autofocus<float>(), src/autofocus/cpu/autofocus_cpu.cpp:250-474, compiled into
+oracle/_ref/libref_pga.so) on seeded defocused images, with the rms values it
+prints per iteration.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # backprojection fixtures
+    python tests/golden/make_golden.py --pga    # PGA fixtures
 """
 from __future__ import annotations
 
@@ -40,10 +45,64 @@ def scene_for(name: str) -> S.Scene:
     return sc
 
 
+PGA_CASES = {
+    # name: (azimuth samples, edge attenuation: columns at each end scaled by 1e-3, iterations)
+    "pga_cpp_64x64": (64, 0, 4),
+    "pga_cpp_64x63_edges": (63, 6, 12),
+}
+
+
+def pga_input(n: int, edge: int) -> np.ndarray:
+    """A seeded point-target image (FP64 oracle, 64 range lines) defocused by a
+    quadratic + cubic azimuth phase error; `edge` columns at each azimuth end
+    attenuated 60 dB so that the -30 dB window of PGA cuts them."""
+    sc = S.point_target_scene(K=64, Np=64, n=64, spacing=0.12, nfft=512, snr_db=30.0, seed=12, n_targets=4,
+                              extent=5.0)
+    img = O.focus_fp64(sc)[0][:, :n].astype(np.complex128)
+    x = np.linspace(-1.0, 1.0, n)
+    phi = 4.0 * x ** 2 + 1.5 * x ** 3
+    img = np.fft.ifft(np.fft.fft(img, axis=1) * np.exp(1j * phi)[None, :], axis=1)
+    if edge:
+        img[:, :edge] *= 1e-3
+        img[:, n - edge:] *= 1e-3
+    return img.astype(np.complex64)
+
+
+def run_ref_pga(img: np.ndarray, iters: int):
+    """The reference's compiled autofocus<float>() on img, with the rms values
+    it prints captured from file descriptor 1."""
+    import tempfile
+
+    sys.stdout.flush()
+    saved = os.dup(1)
+    with tempfile.TemporaryFile(mode="w+") as tmp:
+        os.dup2(tmp.fileno(), 1)
+        try:
+            out = O.ref_pga(img, iters)
+        finally:
+            os.dup2(saved, 1)
+            os.close(saved)
+        tmp.seek(0)
+        rms = [float(line.split("=")[1]) for line in tmp.read().splitlines() if line.startswith("rms =")]
+    return out, np.asarray(rms)
+
+
+def write_pga(out_dir: str) -> None:
+    for name, (n, edge, iters) in PGA_CASES.items():
+        img = pga_input(n, edge)
+        out, rms = run_ref_pga(img, iters)
+        np.savez_compressed(os.path.join(out_dir, name + ".npz"), image=img, iterations=iters, ref_out=out,
+                            ref_rms=rms)
+        print(name, "written", len(rms), "iterations")
+
+
 def main() -> None:
     if not O.ref_available():
         O.build()
     out_dir = os.path.dirname(os.path.abspath(__file__))
+    if "--pga" in sys.argv:
+        write_pga(out_dir)
+        return
     for name in CASES:
         sc = scene_for(name)
         img32, maxwy32, sf32 = O.reference_focus(sc, "f32")

@@ -91,3 +91,56 @@ def test_captured_descent_matches_eager(torch_cuda):
         re_, he, _ = AF.line_of_sight_autofocus(plan, ax, ay, az, r0, f0, iters=15, graph=False)
         assert np.allclose([h["entropy"] for h in hg], [h["entropy"] for h in he], rtol=1e-6, atol=0)
         assert torch.allclose(rg, re_, rtol=0, atol=1e-9)
+
+
+def test_reference_costs_on_the_gpu_match_the_transcriptions(torch_cuda):
+    """The reference's two grid-search costs, batched on the device, against
+    direct transcriptions of the reference's loops (dft2DCalculation,
+    gridSearchErrorFunctions_dft.cuh:112-203,320-335; cuCalculateColumnEntropy,
+    gridSearchErrorFunctions.cuh:341-447) run on the CPU."""
+    torch = torch_cuda
+    from uncc_sar_focusing_b200 import autofocus as AF
+
+    import test_autofocus as T
+
+    rng = np.random.default_rng(8)
+    imgs = (rng.standard_normal((3, 12, 10)) + 1j * rng.standard_normal((3, 12, 10))).astype(np.complex64)
+    imgs[2, 5, :] = 0.0
+    dft = AF.reference_dft_costs(torch.as_tensor(imgs).cuda()).cpu().numpy()
+    col = AF.reference_column_entropies(torch.as_tensor(imgs).cuda()).cpu().numpy()
+    for i in range(3):
+        u8 = AF.reference_u8_image(torch.as_tensor(imgs[i])).numpy().astype(np.float64)
+        nx, ny = u8.shape
+        hh, hw = ny // 2, nx // 2
+        threshold = int((hh * hh + hw * hw) * (0.35 * 0.35))
+        out = 0.0
+        for dft_x in range(nx):
+            d1 = [sum(u8[x, yy] * np.exp(-2j * np.pi * dft_x * x / nx) for x in range(nx)) for yy in range(ny)]
+            d2 = [sum(np.exp(-2j * np.pi * dy * yy / ny) * d1[yy] for yy in range(ny)) for dy in range(ny)]
+            for y in range(hh):
+                if dft_x * dft_x + y * y < threshold or (nx - dft_x - 1) ** 2 + y * y < threshold:
+                    out += abs(d2[y]) + abs(d2[ny - y - 1])
+        assert abs(dft[i] + out) < 1e-6 * out
+        assert abs(col[i] - T.column_entropy_transcription(imgs[i])) < 1e-9
+
+
+def test_grid_search_with_the_reference_cost_improves_focus(torch_cuda):
+    torch = torch_cuda
+    from uncc_sar_focusing_b200 import autofocus as AF
+    from uncc_sar_focusing_b200 import focusing
+
+    sc = S.motion_error_scene(K=128, Np=256, n=96, spacing=0.16, peak=0.3, walk_sigma=0.0, seed=11,
+                              device="cuda")
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    ax, ay, az, r0, f0 = (dev(v) for v in (sc.ant_x, sc.ant_y, sc.ant_z, sc.slant_range, sc.start_freq))
+    with focusing.Plan.for_scene(sc, "mixed") as plan:
+        plan.range_compress(dev(sc.phase_history))
+        motion = AF.CubicMotion(ax, ay, az)
+        before = AF.focus_metrics(plan.backproject(ax, ay, az, r0, f0))
+        res = AF.grid_search_autofocus(plan, motion, r0, f0, span=0.3, points=3, levels=3, batch=243)
+        a = motion.track(res.theta)
+        after = AF.focus_metrics(plan.backproject(a[0].contiguous(), a[1].contiguous(), a[2].contiguous(), r0, f0))
+    assert res.images_formed == 3 * 3 ** 6
+    assert [h["cost"] for h in res.history] == ["reference_dft"] * 3
+    assert after["reference_dft_cost"] < before["reference_dft_cost"]
+    assert abs(after["reference_dft_cost"] - res.history[-1]["score"]) < 1e-6 * abs(after["reference_dft_cost"])
