@@ -347,14 +347,26 @@ def autofocus_section(dev, grid_seconds: float):
         AF.focus_motion_error(plan, ax, ay, az, r0, f0, cubic_iters=5, los_iters=5, pga_iters=1)  # warm-up
         grad = AF.focus_motion_error(plan, ax, ay, az, r0, f0)
         motion = AF.CubicMotion(ax, ay, az)
-        grid = AF.grid_search_autofocus(plan, motion, r0, f0, span=1.5, points=5, levels=4, batch=128,
-                                        deadline_s=grid_seconds, cost="reference_dft")
-        a = motion.track(grid.theta)
-        img_grid = plan.backproject(a[0].contiguous(), a[1].contiguous(), a[2].contiguous(), r0, f0)
-        metrics_grid = AF.focus_metrics(img_grid)
+        searches = {}
+        for cost in ("reference_dft", "entropy"):
+            g = AF.grid_search_autofocus(plan, motion, r0, f0, span=1.5, points=5, levels=4, batch=128,
+                                         deadline_s=grid_seconds, cost=cost)
+            a = motion.track(g.theta)
+            img_g = plan.backproject(a[0].contiguous(), a[1].contiguous(), a[2].contiguous(), r0, f0)
+            searches[cost] = (g, AF.focus_metrics(img_g))
         metrics_grad = AF.focus_metrics(grad["image"])
-    e_grid = metrics_grid["shannon_entropy"]
-    t_grad = AF.time_to_entropy(grad["timeline"], e_grid)
+
+    def search_entry(cost):
+        g, metrics = searches[cost]
+        e = metrics["shannon_entropy"]
+        t = AF.time_to_entropy(grad["timeline"], e)
+        return {"cost": cost, "entropy": e, "seconds": g.seconds, "images": g.images_formed,
+                "levels_done": len(g.history), "bounded_to_s": grid_seconds, "final_image": metrics,
+                "searched": "slope and quadratic term of each axis (the reference's quadratic search without "
+                            "its velocity scale), 5 points each, box halved per level; the 12 cubic coefficients "
+                            "at 5 points would be 5^12 images per level",
+                "sec_to_focus": {"target_entropy": e, "gradient_s": t, "grid_search_s": g.seconds,
+                                 "speedup": (g.seconds / t) if t else None}}
     return {
         "workload": "autofocus: 9.6 GHz / 600 MHz, 4 deg at 10 km, 30 deg el, 1024 pulses x 512 samples, 512^2 "
                     "image at 0.08 m, 5 targets, 20 dB SNR; track error per axis = seeded cubic (1.5 m peak) + "
@@ -366,14 +378,16 @@ def autofocus_section(dev, grid_seconds: float):
                      "stages": "Adam on 12 cubic coefficients (300 it) -> Adam on 1024 per-pulse ranges "
                                "(200 it) -> PGA (PGA.m semantics, on the device); gradients from the adjoint "
                                "kernel"},
-        "grid_search": {"cost": "reference_dft", "entropy": e_grid, "seconds": grid.seconds,
-                        "images": grid.images_formed, "levels_done": len(grid.history),
-                        "bounded_to_s": grid_seconds, "final_image": metrics_grid,
-                        "searched": "slope and quadratic term of each axis (the reference's quadratic search "
-                                    "without its velocity scale), 5 points each, box halved per level; the 12 "
-                                    "cubic coefficients at 5 points would be 5^12 images per level"},
-        "sec_to_focus": {"target_entropy": e_grid, "gradient_s": t_grad, "grid_search_s": grid.seconds,
-                         "speedup": (grid.seconds / t_grad) if t_grad else None},
+        # the reference's own method: every grid point scored with its DFT
+        # cost; that cost rewards low-frequency energy of the 8-bit image, so
+        # its optimum need not be the sharpest image
+        "grid_search": search_entry("reference_dft"),
+        # the same search scored with the gradient pipeline's objective
+        "grid_search_entropy": search_entry("entropy"),
+        # headline: time for the gradient pipeline to reach the final Shannon
+        # entropy of the stronger of the two searches
+        "sec_to_focus": min((search_entry(c)["sec_to_focus"] for c in searches),
+                            key=lambda d: d["target_entropy"]),
     }
 
 
