@@ -72,6 +72,21 @@ def check_scene(scene, mx):
                 f = np.floor(Bx[active])
                 worst_lo = min(worst_lo, f.min())
                 worst_hi = max(worst_hi, f.max())
+            # each pulse's tight window (make_geo, bp_tile.cuh): half-width
+            # wp = min(W, ceil(|gam| TX/2 + |eta| 32 + lam hd^2 / (2 (Rc - hd))) + 3)
+            # (W for near-field pulses), copied to entries [W - wp, W + wp + 2)
+            k = 2.0 * scene.start_freq / 299792458.0
+            near = (rc < 16 * P["hd"]) | (rc ** 3 < k * 0.625 * P["hd"] ** 4 / 1e-7)
+            gam, eta = -P["lam"] * u[:, 0] * P["dx"], -P["lam"] * u[:, 1] * P["dy"]
+            span = np.abs(gam) * (TX // 2) + np.abs(eta) * 32 + P["lam"] * P["hd"] ** 2 / (2 * (rc - P["hd"]))
+            wp = np.where(near | (span >= P["W"]), P["W"], np.minimum(P["W"], np.ceil(span).astype(np.int64) + 3))
+            for Bx in (B, B2):
+                f = np.floor(Bx)[active]
+                lo_ok = f >= (P["W"] - wp)[active, None, None]
+                hi_ok = f <= (P["W"] + wp)[active, None, None]
+                assert lo_ok.all() and hi_ok.all(), "a pixel's bin falls outside its pulse's tight window"
+            tight_frac = float(np.mean((2 * wp + 2) / P["wsize"]))
+            P["tight_frac"] = min(P.get("tight_frac", 1.0), tight_frac)
     assert worst_lo >= 0, worst_lo
     assert worst_hi <= P["wsize"] - 2, (worst_hi, P["wsize"])
     return worst_lo, worst_hi, P
@@ -89,7 +104,17 @@ def test_large_config_indices(mx):
     sc = S.large_scene(K=64, Np=48, n=1024, n_targets=1)
     sc.nfft = 8 * 1024  # the large configuration's range sampling (max_wr from 640 MHz over 1024 samples)
     sc.delta_freq = 640e6 / 1023
-    check_scene(sc, mx)
+    _, _, P = check_scene(sc, mx)
+    if mx == 8:
+        assert P["tight_frac"] < 0.7  # the tight windows copy and rewrite about 40% fewer entries
+
+
+def test_volumetric_config_indices():
+    sc = S.volumetric_scene(K=16, pulses_per_pass=24, elevations=(30.0, 31.4), nx=256, ny=256, nz=1,
+                            n_targets=1)
+    sc.nfft = 8 * 512
+    sc.delta_freq = 600e6 / 511
+    check_scene(sc, 8)
 
 
 def test_swath_edge_and_odd_grid_indices():
@@ -211,3 +236,37 @@ def test_unit_cursor_matches_division():
                             if iz == nz:
                                 iz, hyp = 0, hyp + 1
                 cur = [b, ty, tx, iz, hyp]
+
+
+def stage_rotation(t, stages, units, G):
+    """SceneCursor::set_rot (bp_mixed.cu): unit t S + b of tile t processes
+    pulse stage (b + rot_t) mod S, rot_t = t S - lo(owner of unit t S)."""
+    first = t * stages
+    return (first - sk_lo(sk_owner(first, units, G), units, G)) % stages
+
+
+@pytest.mark.parametrize("tiles,stages,G", [
+    (256, 256, 296), (512, 256, 296), (1024, 256, 296), (32, 64, 296), (17, 5, 17), (3, 3, 9), (7, 1, 3),
+    (8192, 128, 296), (256, 256, 256),
+])
+def test_stage_rotation_walks_resident_ctas_in_step(tiles, stages, G):
+    """Every tile still processes each of its pulse stages exactly once, and
+    a CTA works on stage k mod S at its local step k, except on its first
+    (partial) tile, which runs lo(c) - lo(owner of that tile) stages off: the
+    CTAs resident together stage nearby pulses through L2."""
+    units = tiles * stages
+    G = min(G, units)
+    for t in range(tiles):
+        r = stage_rotation(t, stages, units, G)
+        assert sorted((b + r) % stages for b in range(stages)) == list(range(stages))
+    for c in range(G):
+        lo, hi = sk_lo(c, units, G), sk_lo(c + 1, units, G)
+        for k, u in enumerate(range(lo, hi)):
+            t, b = divmod(u, stages)
+            stage = (b + stage_rotation(t, stages, units, G)) % stages
+            off = (stage - k) % stages
+            owner = sk_owner(t * stages, units, G)
+            if owner == c:
+                assert off == 0
+            else:
+                assert k < stages and off == (lo - sk_lo(owner, units, G)) % stages

@@ -129,6 +129,7 @@ void release(sarbp_plan *p) {
     cudaFree(p->d_gout);
     cudaFree(p->d_hyp);
     cudaFree(p->d_sk);
+    cudaFree(p->d_geotab);
     cudaFree(p->d_rctab);
     cudaFree(p->d_win);
     delete p;
@@ -244,6 +245,8 @@ BpLaunch launch_params(const sarbp_plan *p, const double *ax, const double *ay, 
     L.sk_partial = p->d_sk;
     L.sk_slot_bytes = static_cast<long long>(p->sk_bytes);
     L.sk_resident = p->sk_resident;
+    L.geo_tab = p->d_geotab;
+    L.geo_tab_records = p->geotab_records;
     return L;
 }
 
@@ -692,6 +695,17 @@ int sarbp_plan_create(const sarbp_plan_desc *desc, sarbp_plan **out) {
             p->sk_bytes = sk;
         } else {
             p->sk_resident = 0;
+        }
+    }
+    // geometry records of a single-image launch from a pre-pass kernel
+    // (environment SARBP_PREGEO=0: computed by the producing lanes instead)
+    if (p->precision == SARBP_PRECISION_MIXED) {
+        const char *env = std::getenv("SARBP_PREGEO");
+        if (!(env && std::strcmp(env, "0") == 0)) {
+            const long long recs = static_cast<long long>((g.ny + 63) / 64) *
+                                   ((g.nx + 8 * p->tile.mx - 1) / (8 * p->tile.mx)) * g.nz * p->np_cap;
+            if (alloc(p, &p->d_geotab, static_cast<size_t>(recs) * sizeof(PulseGeo)) == SARBP_OK)
+                p->geotab_records = recs;
         }
     }
     if (cudaMemset(p->d_pairs, 0, np * static_cast<size_t>(p->row_stride) * entry) != cudaSuccess ||

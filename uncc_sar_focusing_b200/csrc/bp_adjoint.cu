@@ -484,6 +484,8 @@ cudaError_t launch_bp_adjoint(const BpLaunch &L, const void *grad, void *partial
     if (tc.mx == MX_ && tc.pb == PB_) return launch_adj<MX_, PB_>(L, grad, partials, smem, s);
     SARBP_ADJ_CASE(8, 8)
     SARBP_ADJ_CASE(8, 4)
+    SARBP_ADJ_CASE(8, 2)  // wide windows: the stage depth halves below 4 at 64-row tiles too
+    SARBP_ADJ_CASE(8, 1)
     SARBP_ADJ_CASE(4, 8)
     SARBP_ADJ_CASE(2, 8)
     SARBP_ADJ_CASE(1, 8)

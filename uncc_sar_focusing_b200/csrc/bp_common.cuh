@@ -116,9 +116,10 @@ struct __align__(16) PulseGeo {
     float a8r, b32r, g8, e32;  // 2 pi frac(8 alpha), 2 pi frac(32 beta) (rad); 8 gam, 32 eta (bins)
     float tx, ty, h, hr;     // ux dx, uy dy (m); 1/(2 Rc), 1/(2 Rc^2)
     float kr, rc, lo, hi;    // 2 pi k (rad/m); Rc; valid iff lo < B_rel < hi
-    int ws;                  // window start bin (may be negative: guard band)
+    int ws;                  // start bin of the tile's full window (W bins each side; may be negative)
     int flags;               // PG_*
-    int pad0, pad1;
+    int wp;                  // this pulse's half-width (<= W): the bins it can reach from the tile
+    int pad1;
     float ux, uy, uz, rinv;  // unit vector tile centre -> antenna, 1/Rc (adjoint kernel)
 };
 static_assert(sizeof(PulseGeo) == 128, "PulseGeo layout");

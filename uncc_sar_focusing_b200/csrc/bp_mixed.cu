@@ -56,6 +56,14 @@ constexpr int kFastUnroll = SARBP_FAST_UNROLL;
 #endif
 constexpr int kCtasPerSm = SARBP_CTAS_PER_SM;
 
+constexpr int kTabEntries = kBaseEntries;
+
+// pulse stages of split tiles walked in step across the resident CTAs
+#ifndef SARBP_STAGE_ROTATION
+#define SARBP_STAGE_ROTATION 1
+#endif
+constexpr bool kRotate = SARBP_STAGE_ROTATION != 0;
+
 
 // One pulse into the thread's MX x 2 pixels.  The two columns l = 0, 1 (32 apart) of a
 // row form a pair and their geometry arithmetic and complex
@@ -121,8 +129,10 @@ __device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, const float4
                 addr = valid ? addr : zero_addr;
             }
             if (CHECKED) {
-                const uint32_t idx = __float_as_uint(yl) - kRoundMagicBits + static_cast<uint32_t>(W);
-                if (idx > static_cast<uint32_t>(wsize - 2)) {
+                // entry floor(B) + W must lie in the pulse's tight window
+                // [W - wp, W + wp] (its next entry too)
+                const uint32_t idx = __float_as_uint(yl) - kRoundMagicBits + static_cast<uint32_t>(g.wp);
+                if (idx > static_cast<uint32_t>(2 * g.wp)) {
                     atomicOr(err, ERRBIT_BOUNDS);
                     addr = zero_addr;
                 }
@@ -188,14 +198,34 @@ __device__ __forceinline__ int slot_pair(int warp, int lane, int k) { return (wa
 
 // Unit cursor over one launch (BATCH = false: the kernel parameter's scene)
 // or over the scenes of a batch table, scene-major.
+//
+// Pulse-stage order within a tile (single-scene launches split over the
+// resident CTAs): unit t S + b of tile t processes stage (b + rot_t) mod S
+// with rot_t = t S - lo(owner of unit t S) mod S, the local step at which
+// that CTA reaches the tile.  A CTA's k-th unit then works on stage k mod S,
+// except on its first, partial tile, so the CTAs resident together walk the
+// pulses in step and share the range profiles they stage through L2.  For
+// the tiles a CTA reaches at their first stage rot_t = -lo(c) mod S, one
+// value per CTA (rot_later); only the first tile has its own.  Every stage
+// of a tile is still processed exactly once; only the order of the per-tile
+// sums changes.
 template <int TX, int PB, bool BATCH>
 struct SceneCursor {
     const BpLaunch *L;
     TileGrid g;
     UnitCursor u;
     int scene;
+    int rot;  // stage rotation of the current tile
 
-    __device__ __forceinline__ void init(const BpLaunch *L0, const BatchScene *scenes, int nscenes, long long unit) {
+    // pulse stage of the current unit
+    __device__ __forceinline__ int stage() const {
+        const int e = u.b + rot;
+        return e >= g.stages ? e - g.stages : e;
+    }
+
+    // cursor at `unit` of U units split over the launch's G = gridDim.x CTAs
+    __device__ __forceinline__ void init(const BpLaunch *L0, const BatchScene *scenes, int nscenes, long long unit,
+                                         long long U) {
         scene = 0;
         L = L0;
         if constexpr (BATCH) {
@@ -211,10 +241,18 @@ struct SceneCursor {
         }
         g = tile_grid(*L, TX, PB);
         u.init(g, *L, unit);
+        rot = 0;
+        if constexpr (!BATCH && kRotate) {
+            const long long G = gridDim.x;
+            const long long first = unit - u.b;  // the tile's first unit
+            rot = static_cast<int>((first - sk_lo(sk_owner(first, U, G), U, G)) % g.stages);
+        }
     }
-    // true when the cursor moved on to the next scene
-    __device__ __forceinline__ bool advance(const BatchScene *scenes, int nscenes) {
+    // true when the cursor moved on to the next scene; rot_later: the stage
+    // rotation of tiles entered at their first stage
+    __device__ __forceinline__ bool advance(const BatchScene *scenes, int nscenes, int rot_later) {
         u.advance(g, *L);
+        if (u.b == 0) rot = rot_later;
         if constexpr (BATCH) {
             if (u.hyp >= L->nhyp && scene + 1 < nscenes) {
                 ++scene;
@@ -242,7 +280,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
     float4 *zero = reinterpret_cast<float4 *>(smem + 16);
     PulseGeo *geo = reinterpret_cast<PulseGeo *>(smem + 32);
     float4 *bases = reinterpret_cast<float4 *>(smem + 32 + 2 * PB * sizeof(PulseGeo));
-    const uint32_t win_addr = smem_addr(smem + 32 + 2 * PB * (sizeof(PulseGeo) + kBaseEntries * sizeof(float4)));
+    const uint32_t win_addr = smem_addr(smem + 32 + 2 * PB * (sizeof(PulseGeo) + kTabEntries * sizeof(float4)));
     const uint32_t zero_addr = smem_addr(zero);
     const uint32_t buf_bytes = static_cast<uint32_t>(PB) * static_cast<uint32_t>(L0.wsize) * 16u;
 
@@ -269,7 +307,10 @@ __global__ void __launch_bounds__(kThreads, MINB)
     const int j0 = lane - kTY / 2;  // column offset of the first pixel (the second is 32 on)
 
     SceneCursor<TX, PB, BATCH> cc, pc;  // consumer at unit i, producer at unit i + 1
-    cc.init(&L0, scenes, nscenes, lo);
+    cc.init(&L0, scenes, nscenes, lo, U);
+    // stage rotation of the tiles this CTA enters at their first stage
+    const int rot_later =
+        (!BATCH && kRotate) ? static_cast<int>((cc.g.stages - lo % cc.g.stages) % cc.g.stages) : 0;
     pc = cc;
 
     // per-scene constants of the consumer
@@ -315,9 +356,16 @@ __global__ void __launch_bounds__(kThreads, MINB)
         const double cx = L.left + static_cast<double>(pc.u.tx * TX + TX / 2) * L.dx;
         const double cy = L.bottom + static_cast<double>(pc.u.ty * kTY + kTY / 2) * L.dy;
         const double cz = L.zlow + static_cast<double>(pc.u.iz) * L.dz;
-        produce_slots<PB>(L, pc.u.b, geo + s * PB, bases + s * PB * kBaseEntries, win_addr + s * buf_bytes,
+        const PulseGeo *pre = nullptr;
+        if (!BATCH && L.geo_tab) {
+            const long long t =
+                ((static_cast<long long>(pc.u.hyp) * L.nz + pc.u.iz) * pc.g.tiles_x + pc.u.tx) * pc.g.tiles_y +
+                pc.u.ty;
+            pre = static_cast<const PulseGeo *>(L.geo_tab) + t * L.np;
+        }
+        produce_slots<PB>(L, pc.stage(), geo + s * PB, bases + s * PB * kTabEntries, win_addr + s * buf_bytes,
                           bar_base + 8 * s, warp, lane, TX / 2, cx, cy,
-                          cz, static_cast<long long>(pc.u.hyp) * L.np);
+                          cz, static_cast<long long>(pc.u.hyp) * L.np, pre);
     };
 
     produce(0);
@@ -330,16 +378,16 @@ __global__ void __launch_bounds__(kThreads, MINB)
     for (int i = 0; i < n; ++i) {
         const int s = i & 1;
         if (i + 1 < n) {
-            pc.advance(scenes, nscenes);
+            pc.advance(scenes, nscenes, rot_later);
             produce(s ^ 1);
             last_issued = i + 1;
         }
         const BpLaunch &L = *cc.L;
         const int S = cc.g.stages;
-        const int b = cc.u.b;
+        const int b = cc.u.b;  // position in the tile's stage order
         const bool ok = mbar_wait_bounded(bar_base + 8 * s, (i >> 1) & 1, L.err);
         if (ok) {
-            const int nq = min(PB, L.np - b * PB);
+            const int nq = min(PB, L.np - cc.stage() * PB);
             // stage summary: all PB pulses active, none gated or near-field
             const int my_flags = lane < nq ? geo[s * PB + lane].flags : 0;
             const int any_f = __reduce_or_sync(0xffffffffu, my_flags);
@@ -351,13 +399,13 @@ __global__ void __launch_bounds__(kThreads, MINB)
                 constexpr int kUnroll = kFastUnroll > 0 ? kFastUnroll : (MX >= 8 && PB >= 8 ? 4 : PB);
 #pragma unroll kUnroll
                 for (int q = 0; q < PB; ++q)
-                    accumulate_pulse<MX, false, false, CHECKED>(geo[s * PB + q], bases + (s * PB + q) * kBaseEntries,
+                    accumulate_pulse<MX, false, false, CHECKED>(geo[s * PB + q], bases + (s * PB + q) * kTabEntries,
                                                                 w0 + q * pulse_bytes, zero_addr, warp, lane, lam,
                                                                 nd2, acc_re, acc_im, wsize, L.W, L.err);
             } else {
                 for (int q = 0; q < nq; ++q) {
                     const PulseGeo &g = geo[s * PB + q];
-                    const float4 *bq = bases + (s * PB + q) * kBaseEntries;
+                    const float4 *bq = bases + (s * PB + q) * kTabEntries;
                     const int flags = g.flags;
                     if (!(flags & PG_ACTIVE)) continue;
                     const uint32_t w = w0 + q * pulse_bytes;
@@ -408,7 +456,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
             ++seg;
             seg_first = 0;
         }
-        if (cc.advance(scenes, nscenes)) scene_consts();
+        if (cc.advance(scenes, nscenes, rot_later)) scene_consts();
     }
 }
 
@@ -469,14 +517,45 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+// Geometry records of every (tile, pulse) of a launch, [tile][pulse], one
+// thread each (make_geo, full warps), for the forward kernel's producers to
+// load.
+template <int MX>
+__global__ void __launch_bounds__(256) bp_geo_records_kernel(const __grid_constant__ BpLaunch L, long long n) {
+    constexpr int TX = 8 * MX;
+    const TileGrid tg = tile_grid(L, TX, 1);
+    PulseGeo *out = static_cast<PulseGeo *>(L.geo_tab);
+    for (long long i = blockIdx.x * 256ll + threadIdx.x; i < n; i += static_cast<long long>(gridDim.x) * 256) {
+        const long long t = i / L.np;
+        const int p = static_cast<int>(i - t * L.np);
+        int tx0, ty0, zz;
+        tile_origin(tg, t, TX, tx0, ty0, zz);
+        const int hyp = zz / L.nz, iz = zz - hyp * L.nz;
+        const double cx = L.left + static_cast<double>(tx0 + TX / 2) * L.dx;
+        const double cy = L.bottom + static_cast<double>(ty0 + kTY / 2) * L.dy;
+        const double cz = L.zlow + static_cast<double>(iz) * L.dz;
+        out[i] = make_geo(L, p, static_cast<long long>(hyp) * L.np, cx, cy, cz, TX / 2);
+    }
+}
+
 template <int MX, int PB, bool CHECKED, int MINB>
-cudaError_t launch_kernels(const BpLaunch &L, size_t smem, cudaStream_t s) {
+cudaError_t launch_kernels(const BpLaunch &L0, size_t smem, cudaStream_t s) {
     constexpr int TX = 8 * MX;
     auto kern = bp_mixed_kernel<MX, PB, CHECKED, MINB, false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    const TileGrid tg = tile_grid(L, TX, PB);
+    const TileGrid tg = tile_grid(L0, TX, PB);
     if (tg.units < 1) return cudaSuccess;
+    BpLaunch L = L0;
+    const long long nrec = tg.tiles * L.np;
+    if (L.geo_tab && nrec <= L.geo_tab_records) {
+        const long long blocks = (nrec + 255) / 256;
+        bp_geo_records_kernel<MX><<<static_cast<unsigned>(blocks < 148 * 64 ? blocks : 148 * 64), 256, 0, s>>>(L, nrec);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    } else {
+        L.geo_tab = nullptr;
+    }
     // split the units over the resident CTAs unless the tiles fill whole waves
     long long G = tg.tiles;
     if (L.sk_partial && L.sk_resident > 0 && tg.tiles % L.sk_resident != 0) {
@@ -565,7 +644,7 @@ int batch_resident_mx_pb(size_t smem) {
 }  // namespace
 
 size_t bp_mixed_smem_bytes(const TileConfig &tc, int wsize) {
-    return 32 + 2 * static_cast<size_t>(tc.pb) * (sizeof(PulseGeo) + kBaseEntries * sizeof(float4)) +
+    return 32 + 2 * static_cast<size_t>(tc.pb) * (sizeof(PulseGeo) + kTabEntries * sizeof(float4)) +
            2 * static_cast<size_t>(tc.pb) * static_cast<size_t>(wsize) * 16;
 }
 

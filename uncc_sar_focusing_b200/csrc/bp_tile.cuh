@@ -100,18 +100,44 @@ struct UnitCursor {
     }
 };
 
+#ifndef SARBP_GEO_RSQ
+#define SARBP_GEO_RSQ 1
+#endif
+
+// 1/sqrt(s) in double by Newton-Raphson for the reciprocal square root,
+// y <- y (3 - s y^2) / 2, from the single-precision hardware estimate (about
+// 2^-22 relative): each step squares the relative error, two reach double
+// precision.  In place of a double sqrt and a double division on the
+// producing lane, whose instruction sequences are several times longer.
+__device__ __forceinline__ double rsqrt_newton(double s) {
+    double y = static_cast<double>(rsqrtf(static_cast<float>(s)));
+    const double hs = 0.5 * s;
+    y = y * fma(-hs * y, y, 1.5);
+    y = y * fma(-hs * y, y, 1.5);
+    return y;
+}
+
+// tx_half: half the tile's rows (its columns are 64: 32 each side)
 __device__ __forceinline__ PulseGeo make_geo(const BpLaunch &L, int p, long long goff, double cx, double cy,
-                                             double cz) {
+                                             double cz, int tx_half) {
     PulseGeo g;
     g.flags = 0;
     const long long gi = goff + p;  // geometry of hypothesis goff / np
     const double ax = L.ax[gi], ay = L.ay[gi], az = L.az[gi], r0 = L.r0[gi], f0 = L.f0[gi];
     const double vx = ax - cx, vy = ay - cy, vz = az - cz;
+#if SARBP_GEO_RSQ
+    const double s2 = vx * vx + vy * vy + vz * vz;
+    const double inv = rsqrt_newton(s2);
+    const double rc = s2 * inv;
+    constexpr double kTwoOverC = 2.0 / kClight;
+    const double k = f0 * kTwoOverC;
+#else
     const double rc = sqrt(vx * vx + vy * vy + vz * vz);
     const double inv = 1.0 / rc;
+    const double k = 2.0 * f0 / kClight;
+#endif
     const double ux = vx * inv, uy = vy * inv;
     const double D = rc - r0;
-    const double k = 2.0 * f0 / kClight;
     const double bc = D * L.lambda + L.half_nfft;
     const double kd = k * D;
     if (!(isfinite(bc) && isfinite(kd) && isfinite(ux) && isfinite(uy) && rc > 0.0 && fabs(bc) < 1.0e9 &&
@@ -146,10 +172,29 @@ __device__ __forceinline__ PulseGeo make_geo(const BpLaunch &L, int p, long long
     g.uy = static_cast<float>(uy);
     g.uz = static_cast<float>(vz * inv);
     g.rinv = static_cast<float>(inv);
+
     int flags = 0;
-    if (!(ws + L.wsize - 2 <= 0 || ws + 1 >= L.nfft - 1)) flags |= PG_ACTIVE;
-    if (!(ws >= 0 && ws + L.wsize <= L.nfft)) flags |= PG_GATE;
     if (rc < L.near_hd16 || rc * rc * rc < k * L.near_coef) flags |= PG_NEAR;
+    // Tight window: a pixel (i, j) of the tile has bin - bc = i gam + j eta +
+    // lambda g with 0 <= g <= hd^2 / (2 (Rc - hd)) (hd the tile
+    // half-diagonal), |i| <= tx_half, |j| <= 32, so its floor(bin) and
+    // floor(bin) + 1 lie within floor(bc) -/+ (ceil(span) + 1): wp =
+    // ceil(span) + 3, at most W (the triangle-inequality bound |bin - bc| <=
+    // lambda hd the full window is sized for).  Near-field pulses keep W.
+    int wp = L.W;
+    if (!(flags & PG_NEAR)) {
+        const double hd = L.near_hd16 * (1.0 / 16.0);
+        const double span = fabs(g.gam) * tx_half + fabs(g.eta) * 32.0 + L.lambda * hd * hd / (2.0 * (rc - hd));
+        if (span < L.W) {
+            const int w = static_cast<int>(ceil(span)) + 3;
+            wp = w < L.W ? w : L.W;
+        }
+    }
+    g.wp = wp;
+    // the part of the window this pulse copies: bins [wsp, wsp + 2 wp + 2)
+    const int wsp = ws + (L.W - wp), wsz = 2 * wp + 2;
+    if (!(wsp + wsz - 2 <= 0 || wsp + 1 >= L.nfft - 1)) flags |= PG_ACTIVE;
+    if (!(wsp >= 0 && wsp + wsz <= L.nfft)) flags |= PG_GATE;
     g.flags = flags;
     return g;
 }
@@ -175,11 +220,12 @@ constexpr int kBaseEntries = 32 + kWarps;
 template <int PB>
 __device__ __forceinline__ void produce_slots(const BpLaunch &L, int b, PulseGeo *geo_s, float4 *base_s,
                                               uint32_t win_s, uint32_t bar, int warp, int lane, int tx_half,
-                                              double cx, double cy, double cz, long long goff = 0) {
+                                              double cx, double cy, double cz, long long goff = 0,
+                                              const PulseGeo *pre = nullptr) {
     for (int q = warp; q < PB; q += kWarps) {
         const int p = b * PB + q;
         PulseGeo g = {};
-        if (lane == 0 && p < L.np) g = make_geo(L, p, goff, cx, cy, cz);
+        if (lane == 0 && p < L.np) g = pre ? pre[p] : make_geo(L, p, goff, cx, cy, cz, tx_half);
         if (base_s) {
             const unsigned full = 0xffffffffu;
             const double A = __shfl_sync(full, g.A, 0), alpha = __shfl_sync(full, g.alpha, 0);
@@ -203,11 +249,15 @@ __device__ __forceinline__ void produce_slots(const BpLaunch &L, int b, PulseGeo
         if (lane != 0) continue;
         geo_s[q] = g;
         if (g.flags & PG_ACTIVE) {
-            const uint32_t bytes = static_cast<uint32_t>(L.wsize) * 16u;
-            const float4 *src =
-                static_cast<const float4 *>(L.pairs) + static_cast<long long>(p) * L.row_stride + L.guard + g.ws;
+            // the pulse's tight window, at its place inside the slot's full one
+            const int off = L.W - g.wp;
+            const uint32_t bytes = static_cast<uint32_t>(2 * g.wp + 2) * 16u;
+            const float4 *src = static_cast<const float4 *>(L.pairs) + static_cast<long long>(p) * L.row_stride +
+                                L.guard + g.ws + off;
             mbar_arrive_expect_tx(bar, bytes);
-            bulk_copy_g2s(win_s + static_cast<uint32_t>(q) * bytes, src, bytes, bar);
+            bulk_copy_g2s(win_s + (static_cast<uint32_t>(q) * static_cast<uint32_t>(L.wsize) +
+                                   static_cast<uint32_t>(off)) * 16u,
+                          src, bytes, bar);
         } else {
             mbar_arrive(bar);
         }
@@ -246,7 +296,9 @@ __device__ __forceinline__ void intercept_slots(const PulseGeo *geo_s, uint32_t 
     for (int q = warp; q < PB; q += kWarps) {
         if (!(geo_s[q].flags & PG_ACTIVE)) continue;
         const uint32_t w = win_s + static_cast<uint32_t>(q) * static_cast<uint32_t>(wsize) * 16u;
-        for (int n = lane; n < wsize; n += 32) {
+        // the entries the pulse's tight window copied
+        const int wp = geo_s[q].wp;
+        for (int n = W - wp + lane; n < W + wp + 2; n += 32) {
             const uint32_t a = w + static_cast<uint32_t>(n) * 16u;
             const float4 e = lds128(a);
             const float m = static_cast<float>(n - W);

@@ -37,6 +37,12 @@ struct BpLaunch {
     void *sk_partial;
     long long sk_slot_bytes;  // bytes reserved for sk_partial (launch checks the need)
     int sk_resident;          // CTAs of the kernel resident at once on the device (0: do not split)
+    // Geometry records of every (tile, pulse) of the launch written by a
+    // pre-pass kernel ([tile][pulse], one PulseGeo each; the mixed forward kernel's
+    // producing lanes then load them instead of computing them), and the
+    // records the buffer holds; nullptr: computed in the kernel.
+    void *geo_tab;
+    long long geo_tab_records;
 };
 
 // One scene of a batch (sarbp_batch_focus), in device memory.  The forward
@@ -163,6 +169,8 @@ struct sarbp_plan {
     void *d_rctab;    // twiddle table of the fused range compression (null: cuFFT path)
     int rc_R;         // nfft / K of the fused range compression
     int rc_grid;      // its CTAs
+    void *d_geotab;   // pre-pass geometry records (BpLaunch::geo_tab), tiles x np_cap PulseGeo
+    long long geotab_records;
     void *d_sk;       // partial sums of tiles split over CTAs (BpLaunch::sk_partial)
     size_t sk_bytes;
     int sk_resident;  // resident CTAs of the plan's forward kernel
