@@ -58,6 +58,15 @@ constexpr int kCtasPerSm = SARBP_CTAS_PER_SM;
 
 constexpr int kTabEntries = kBaseEntries;
 
+// Dynamic shared memory of the forward kernel: barriers and the zero entry,
+// two stage buffers of PB records, base tables and windows, and two
+// staging slots of PB pre-pass records.
+__host__ __device__ constexpr size_t smem_bytes_of(int pb, int wsize) {
+    return 32 + 2 * static_cast<size_t>(pb) * (sizeof(PulseGeo) + kTabEntries * sizeof(float4)) +
+           2 * static_cast<size_t>(pb) * static_cast<size_t>(wsize) * 16 +
+           2 * static_cast<size_t>(pb) * sizeof(PulseGeo);
+}
+
 // pulse stages of split tiles walked in step across the resident CTAs
 #ifndef SARBP_STAGE_ROTATION
 #define SARBP_STAGE_ROTATION 1
@@ -349,26 +358,52 @@ __global__ void __launch_bounds__(kThreads, MINB)
 
     // records, base tables and windows of the producer cursor's unit into
     // buffer s
-    auto produce = [&](int s) {
+    // Pre-pass records (single-scene launches): the records of the stage
+    // after the producer's are copied asynchronously into the staging ring
+    // (two stages of PB records after the stage buffers' windows) while the
+    // current stage accumulates, so their global-memory latency does not
+    // stall the producing warps.
+    const bool pregeo = !BATCH && L0.geo_tab != nullptr;
+    PulseGeo *stg = reinterpret_cast<PulseGeo *>(smem + smem_bytes_of(PB, L0.wsize) - 2 * PB * sizeof(PulseGeo));
+    // stage after the producer cursor's unit (last: the CTA has no more)
+    auto prefetch_next = [&](int slot, bool last) {
+        if (last) return;
+        const BpLaunch &L = *pc.L;
+        long long t =
+            ((static_cast<long long>(pc.u.hyp) * L.nz + pc.u.iz) * pc.g.tiles_x + pc.u.tx) * pc.g.tiles_y + pc.u.ty;
+        int st;
+        if (pc.u.b + 1 < pc.g.stages) {
+            st = pc.stage() + 1;
+            if (st == pc.g.stages) st = 0;
+        } else {
+            ++t;  // the next tile, entered at its first stage
+            st = rot_later;
+        }
+        prefetch_records<PB>(L, static_cast<const PulseGeo *>(L.geo_tab) + t * L.np, st, stg + slot * PB, warp, lane);
+    };
+    auto produce = [&](int s, const PulseGeo *staged) {
         // every lane of the warp enters: produce_slots gives lane 0 the record
         // and the copy and uses the whole warp (shuffles) for the base tables
         const BpLaunch &L = *pc.L;
         const double cx = L.left + static_cast<double>(pc.u.tx * TX + TX / 2) * L.dx;
         const double cy = L.bottom + static_cast<double>(pc.u.ty * kTY + kTY / 2) * L.dy;
         const double cz = L.zlow + static_cast<double>(pc.u.iz) * L.dz;
-        const PulseGeo *pre = nullptr;
-        if (!BATCH && L.geo_tab) {
-            const long long t =
-                ((static_cast<long long>(pc.u.hyp) * L.nz + pc.u.iz) * pc.g.tiles_x + pc.u.tx) * pc.g.tiles_y +
-                pc.u.ty;
-            pre = static_cast<const PulseGeo *>(L.geo_tab) + t * L.np;
-        }
         produce_slots<PB>(L, pc.stage(), geo + s * PB, bases + s * PB * kTabEntries, win_addr + s * buf_bytes,
-                          bar_base + 8 * s, warp, lane, TX / 2, cx, cy,
-                          cz, static_cast<long long>(pc.u.hyp) * L.np, pre);
+                          bar_base + 8 * s, warp, lane, TX / 2, cx, cy, cz,
+                          static_cast<long long>(pc.u.hyp) * L.np, staged);
     };
 
-    produce(0);
+    if (pregeo) {
+        // stage 0's records now, stage 1's ahead
+        const BpLaunch &L = *pc.L;
+        const long long t =
+            ((static_cast<long long>(pc.u.hyp) * L.nz + pc.u.iz) * pc.g.tiles_x + pc.u.tx) * pc.g.tiles_y + pc.u.ty;
+        prefetch_records<PB>(L, static_cast<const PulseGeo *>(L.geo_tab) + t * L.np, pc.stage(), stg, warp, lane);
+        produce(0, stg);
+        prefetch_next(1, n < 2);
+    } else {
+        produce(0, nullptr);
+    }
     intercept_slots<PB>(geo, win_addr, bar_base, 0, pc.L->wsize, pc.L->W, warp, lane, pc.L->err);
     __syncthreads();
 
@@ -379,7 +414,15 @@ __global__ void __launch_bounds__(kThreads, MINB)
         const int s = i & 1;
         if (i + 1 < n) {
             pc.advance(scenes, nscenes, rot_later);
-            produce(s ^ 1);
+            if (pregeo) {
+                // stage i + 1's records were prefetched into staging slot
+                // (i + 1) & 1; stage i + 2's go to the other one, whose
+                // records stage i's producer read before the last barrier
+                produce(s ^ 1, stg + (s ^ 1) * PB);
+                prefetch_next(s, i + 2 >= n);
+            } else {
+                produce(s ^ 1, nullptr);
+            }
             last_issued = i + 1;
         }
         const BpLaunch &L = *cc.L;
@@ -426,8 +469,10 @@ __global__ void __launch_bounds__(kThreads, MINB)
             intercept_slots<PB>(geo + (s ^ 1) * PB, win_addr + (s ^ 1) * buf_bytes, bar_base + 8 * (s ^ 1),
                                 ((i + 1) >> 1) & 1, pc.L->wsize, pc.L->W, warp, lane, L.err);
         if (__syncthreads_or(!ok)) {
-            // let the copies already issued for the other buffer land before
-            // the CTA's shared memory goes away (again bounded)
+            // let the copies already issued for the other buffer (and the
+            // record prefetches) land before the CTA's shared memory goes
+            // away (again bounded)
+            asm volatile("cp.async.wait_all;" ::: "memory");
             if (threadIdx.x == 0 && last_issued > i)
                 mbar_wait_bounded(bar_base + 8 * (last_issued & 1), (last_issued >> 1) & 1, L.err);
             return;
@@ -643,10 +688,7 @@ int batch_resident_mx_pb(size_t smem) {
 
 }  // namespace
 
-size_t bp_mixed_smem_bytes(const TileConfig &tc, int wsize) {
-    return 32 + 2 * static_cast<size_t>(tc.pb) * (sizeof(PulseGeo) + kTabEntries * sizeof(float4)) +
-           2 * static_cast<size_t>(tc.pb) * static_cast<size_t>(wsize) * 16;
-}
+size_t bp_mixed_smem_bytes(const TileConfig &tc, int wsize) { return smem_bytes_of(tc.pb, wsize); }
 
 int bp_mixed_resident(const TileConfig &tc, size_t smem) {
 #define SARBP_MIXED_CASE(MX_, PB_) \

@@ -217,15 +217,40 @@ constexpr int kBaseEntries = 32 + kWarps;
 // then lane 0 issues the window's bulk copy (or a plain arrival), whose
 // release on the stage's mbarrier also publishes the tables (__syncwarp
 // orders the other lanes' stores before it).
+// Pre-pass records (BpLaunch::geo_tab) of pulse stage b of the tile whose
+// record row is `rec` into a staging slot of shared memory, asynchronously
+// (cp.async, 16 bytes by each of lanes 0..7 of warp q for slot q): issued a
+// stage ahead of produce_slots, which waits for them.
+template <int PB>
+__device__ __forceinline__ void prefetch_records(const BpLaunch &L, const PulseGeo *rec, int b, PulseGeo *stg,
+                                                 int warp, int lane) {
+    for (int q = warp; q < PB; q += kWarps) {
+        const int p = b * PB + q;
+        if (p < L.np && lane < 8) {
+            const uint32_t dst = smem_addr(reinterpret_cast<const float4 *>(stg + q) + lane);
+            const float4 *src = reinterpret_cast<const float4 *>(rec + p) + lane;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+        }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// Records, base tables and window copies of stage b (see below).  stg: the
+// stage's prefetched records (prefetch_records), or nullptr: lane 0 computes
+// them (make_geo).
 template <int PB>
 __device__ __forceinline__ void produce_slots(const BpLaunch &L, int b, PulseGeo *geo_s, float4 *base_s,
                                               uint32_t win_s, uint32_t bar, int warp, int lane, int tx_half,
                                               double cx, double cy, double cz, long long goff = 0,
-                                              const PulseGeo *pre = nullptr) {
+                                              const PulseGeo *stg = nullptr) {
+    if (stg) {
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncwarp();
+    }
     for (int q = warp; q < PB; q += kWarps) {
         const int p = b * PB + q;
         PulseGeo g = {};
-        if (lane == 0 && p < L.np) g = pre ? pre[p] : make_geo(L, p, goff, cx, cy, cz, tx_half);
+        if (lane == 0 && p < L.np) g = stg ? stg[q] : make_geo(L, p, goff, cx, cy, cz, tx_half);
         if (base_s) {
             const unsigned full = 0xffffffffu;
             const double A = __shfl_sync(full, g.A, 0), alpha = __shfl_sync(full, g.alpha, 0);
