@@ -565,21 +565,34 @@ __global__ void __launch_bounds__(kThreads)
 // Geometry records of every (tile, pulse) of a launch, [tile][pulse], one
 // thread each (make_geo, full warps), for the forward kernel's producers to
 // load.
+// Each CTA computes 256 records into shared memory, then writes them out as
+// consecutive 16-byte words (a warp stores 512 contiguous bytes), not as
+// 128-byte structures 128 bytes apart per lane.
 template <int MX>
 __global__ void __launch_bounds__(256) bp_geo_records_kernel(const __grid_constant__ BpLaunch L, long long n) {
     constexpr int TX = 8 * MX;
+    constexpr int kWords = sizeof(PulseGeo) / sizeof(float4);
+    __shared__ PulseGeo recs[256];
     const TileGrid tg = tile_grid(L, TX, 1);
-    PulseGeo *out = static_cast<PulseGeo *>(L.geo_tab);
-    for (long long i = blockIdx.x * 256ll + threadIdx.x; i < n; i += static_cast<long long>(gridDim.x) * 256) {
-        const long long t = i / L.np;
-        const int p = static_cast<int>(i - t * L.np);
-        int tx0, ty0, zz;
-        tile_origin(tg, t, TX, tx0, ty0, zz);
-        const int hyp = zz / L.nz, iz = zz - hyp * L.nz;
-        const double cx = L.left + static_cast<double>(tx0 + TX / 2) * L.dx;
-        const double cy = L.bottom + static_cast<double>(ty0 + kTY / 2) * L.dy;
-        const double cz = L.zlow + static_cast<double>(iz) * L.dz;
-        out[i] = make_geo(L, p, static_cast<long long>(hyp) * L.np, cx, cy, cz, TX / 2);
+    float4 *out = static_cast<float4 *>(L.geo_tab);
+    for (long long i0 = blockIdx.x * 256ll; i0 < n; i0 += static_cast<long long>(gridDim.x) * 256) {
+        const long long i = i0 + threadIdx.x;
+        if (i < n) {
+            const long long t = i / L.np;
+            const int p = static_cast<int>(i - t * L.np);
+            int tx0, ty0, zz;
+            tile_origin(tg, t, TX, tx0, ty0, zz);
+            const int hyp = zz / L.nz, iz = zz - hyp * L.nz;
+            const double cx = L.left + static_cast<double>(tx0 + TX / 2) * L.dx;
+            const double cy = L.bottom + static_cast<double>(ty0 + kTY / 2) * L.dy;
+            const double cz = L.zlow + static_cast<double>(iz) * L.dz;
+            recs[threadIdx.x] = make_geo(L, p, static_cast<long long>(hyp) * L.np, cx, cy, cz, TX / 2);
+        }
+        __syncthreads();
+        const long long words = (n - i0 < 256 ? n - i0 : 256) * kWords;
+        const float4 *src = reinterpret_cast<const float4 *>(recs);
+        for (int w = threadIdx.x; w < words; w += 256) out[i0 * kWords + w] = src[w];
+        __syncthreads();
     }
 }
 

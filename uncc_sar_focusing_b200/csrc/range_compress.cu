@@ -188,7 +188,13 @@ struct RcTable {
     static constexpr int kWn = kTwk2 + K2 / 2;     // W_N^i, i < 32 R
     static constexpr int kWnr = kWn + 32 * R;      // W_{N/32}^i, i < N / 32
     static constexpr int kSize = kWnr + NW;
-    static constexpr int kReg = K + 36;            // shared row of one sub-transform (2 kReg = 8 mod 32)
+    // shared row of one sub-transform.  The pair-row writes read element
+    // (r, m) = (b mod R, b / R) for consecutive b: 16 lanes (one 128-byte
+    // wavefront of 8-byte reads) cover R values of r and 16/R of m, first
+    // bank 2 (r kReg + m) mod 32; kReg = 16/R mod 16 makes these 16
+    // distinct even banks for every R (K + 36, right for R = 4, put r and
+    // r + 4 on the same banks for R = 8)
+    static constexpr int kReg = K + 32 + 16 / R;
     static constexpr size_t kSmem = (static_cast<size_t>(K) + kSize + static_cast<size_t>(R) * kReg) * 8;
 };
 
