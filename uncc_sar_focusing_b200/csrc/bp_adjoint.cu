@@ -61,10 +61,10 @@ __device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, const float4 *b
     const float4 c0 = *reinterpret_cast<const float4 *>(&g.a8r);  // a8r, b32r, g8, e32
     const float4 c1 = *reinterpret_cast<const float4 *>(&g.tx);   // tx, ty, h, hr
     const float4 c2 = *reinterpret_cast<const float4 *>(&g.kr);   // kr, rc, lo, hi
-    const float4 rowv = base[32 + warp], colv = base[lane];
-    const float P00 = rowv.x + colv.x;
-    const float B00 = rowv.y + colv.y;
-    const float t00 = rowv.z + colv.z;
+    const float4 rowv = base[warp];
+    const float P00 = rowv.x + reinterpret_cast<const float *>(base + kWarps)[lane];
+    const float B00 = fmaf(j0f, c0.w * (1.0f / 32.0f), rowv.y);
+    const float t00 = fmaf(j0f, c1.y, rowv.z);
     float2 t2 = make_float2(t00, fmaf(32.0f, c1.y, t00));  // second pixel: 32 columns on
     float2 Pb = make_float2(P00, P00 + c0.y);
     float2 Bb = make_float2(B00, B00 + c0.w);

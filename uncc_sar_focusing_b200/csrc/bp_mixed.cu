@@ -83,7 +83,7 @@ constexpr bool kRotate = SARBP_STAGE_ROTATION != 0;
 // ng = ne (h + t hr) = -g, and the phase / bin add -kr * ng, -lam * ng.
 template <int MX, bool GATE, bool NEAR, bool CHECKED>
 __device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, const float4 *base, uint32_t w_addr,
-                                                 uint32_t zero_addr, int warp, int lane, float lam,
+                                                 uint32_t zero_addr, int warp, int lane, float lam, float j0f,
                                                  const float2 (&nd2)[MX], float (&acc_re)[MX][2],
                                                  float (&acc_im)[MX][2], int wsize, int W, unsigned *err) {
     const float4 c0 = *reinterpret_cast<const float4 *>(&g.a8r);  // a8r, b32r, g8, e32
@@ -92,15 +92,15 @@ __device__ __forceinline__ void accumulate_pulse(const PulseGeo &g, const float4
     // per-thread phase, bin and projection bases: row part + column part,
     // each reduced in FP64 by the producer (|phase| <= 2 pi); the pair's
     // second pixel is 32 columns on
-    const float4 rowv = base[32 + warp], colv = base[lane];
-    const float P00 = rowv.x + colv.x;
-    const float B00 = rowv.y + colv.y;
-    const float t00 = rowv.z + colv.z;
+    const float4 rowv = base[warp];
+    const float P00 = rowv.x + reinterpret_cast<const float *>(base + kWarps)[lane];
+    const float B00 = fmaf(j0f, c0.w * (1.0f / 32.0f), rowv.y);
+    const float t00 = fmaf(j0f, c1.y, rowv.z);
     float2 t2 = make_float2(t00, fmaf(32.0f, c1.y, t00));
     float2 Pb = make_float2(P00, P00 + c0.y);
     float2 Bb = make_float2(B00, B00 + c0.w);
     const float2 TX8 = splat(8.0f * c1.x), A8 = splat(c0.x), G8 = splat(c0.z);
-    const float2 HR = splat(c1.w), H = splat(c1.z), NKR = splat(-c2.x), NLAM = splat(-lam);
+    const float2 HR = splat(c1.w), H = splat(c1.z), NKR = splat(rowv.w), NLAM = splat(-lam);
     const float2 MAGIC = splat(kRoundMagic);
     // B is the window-centred bin; shared address of pair entry floor(B) + W:
     // bits(B + 1.5*2^23, rounded down) * 16 + w_adj (mod 2^32)
@@ -314,6 +314,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
     if (n <= 0) return;
     const int i0 = warp - TX / 2;
     const int j0 = lane - kTY / 2;  // column offset of the first pixel (the second is 32 on)
+    const float j0f = static_cast<float>(j0);
 
     SceneCursor<TX, PB, BATCH> cc, pc;  // consumer at unit i, producer at unit i + 1
     cc.init(&L0, scenes, nscenes, lo, U);
@@ -437,13 +438,13 @@ __global__ void __launch_bounds__(kThreads, MINB)
             const int all_f = __reduce_and_sync(0xffffffffu, lane < nq ? my_flags : PG_ACTIVE);
             const uint32_t w0 = win_addr + s * buf_bytes;
             if (nq == PB && (all_f & PG_ACTIVE) && !(any_f & (PG_GATE | PG_NEAR))) {
-                // 64-row tiles: half-stage unroll (no spill, 1.932 vs 1.942 ms);
-                // shorter tiles: the whole stage (2.250 vs 2.283 ms at 32 rows)
-                constexpr int kUnroll = kFastUnroll > 0 ? kFastUnroll : (MX >= 8 && PB >= 8 ? 4 : PB);
+                // the whole stage unrolled (64-row tiles: 1.762 vs 1.771 ms for a
+                // half-stage unroll, no spill either way; 32 rows: 2.250 vs 2.283 ms)
+                constexpr int kUnroll = kFastUnroll > 0 ? kFastUnroll : PB;
 #pragma unroll kUnroll
                 for (int q = 0; q < PB; ++q)
                     accumulate_pulse<MX, false, false, CHECKED>(geo[s * PB + q], bases + (s * PB + q) * kTabEntries,
-                                                                w0 + q * pulse_bytes, zero_addr, warp, lane, lam,
+                                                                w0 + q * pulse_bytes, zero_addr, warp, lane, lam, j0f,
                                                                 nd2, acc_re, acc_im, wsize, L.W, L.err);
             } else {
                 for (int q = 0; q < nq; ++q) {
@@ -453,13 +454,13 @@ __global__ void __launch_bounds__(kThreads, MINB)
                     if (!(flags & PG_ACTIVE)) continue;
                     const uint32_t w = w0 + q * pulse_bytes;
                     if (flags & PG_NEAR)
-                        accumulate_pulse<MX, true, true, CHECKED>(g, bq, w, zero_addr, warp, lane, lam, nd2, acc_re,
-                                                                  acc_im, wsize, L.W, L.err);
+                        accumulate_pulse<MX, true, true, CHECKED>(g, bq, w, zero_addr, warp, lane, lam, j0f, nd2,
+                                                                  acc_re, acc_im, wsize, L.W, L.err);
                     else if (flags & PG_GATE)
-                        accumulate_pulse<MX, true, false, CHECKED>(g, bq, w, zero_addr, warp, lane, lam, nd2, acc_re,
-                                                                   acc_im, wsize, L.W, L.err);
+                        accumulate_pulse<MX, true, false, CHECKED>(g, bq, w, zero_addr, warp, lane, lam, j0f, nd2,
+                                                                   acc_re, acc_im, wsize, L.W, L.err);
                     else
-                        accumulate_pulse<MX, false, false, CHECKED>(g, bq, w, zero_addr, warp, lane, lam, nd2,
+                        accumulate_pulse<MX, false, false, CHECKED>(g, bq, w, zero_addr, warp, lane, lam, j0f, nd2,
                                                                     acc_re, acc_im, wsize, L.W, L.err);
                 }
             }

@@ -202,14 +202,15 @@ __device__ __forceinline__ PulseGeo make_geo(const BpLaunch &L, int p, long long
 // Pulse slots of block b handled by this warp (slot q = warp, warp + 8, ...):
 // lane 0 writes the geometry record and either arrives with the window's byte
 // count and issues its bulk copy, or just arrives (inactive / past the end).
-// Per-(tile, pulse) base tables of the mixed forward kernel: entry lane
-// (0..31) is the column part for j0 = lane - 32 (a lane's pixels are columns
-// lane and lane + 32 of the tile) and entry 32 + warp (0..7)
-// the row part for i0 = warp - TX/2 of the thread's phase, bin and
-// projection bases: (2 pi frac(j0 beta), j0 eta, j0 ty, 0) and
-// (2 pi frac(A + i0 alpha), B0 + i0 gam, i0 tx, 0), the phase parts reduced
-// modulo one revolution in FP64.  A thread's base is row + column.
-constexpr int kBaseEntries = 32 + kWarps;
+// Per-(tile, pulse) base tables of the mixed kernels (forward and adjoint),
+// kBaseEntries float4 words: row entries 0..7, one per warp, for
+// i0 = warp - TX/2: (2 pi frac(A + i0 alpha), B0 + i0 gam, i0 tx, -kr), then
+// 32 floats, one per lane, for j0 = lane - 32 (a lane's pixels are columns
+// lane and lane + 32 of the tile): the column phase 2 pi frac(j0 beta).  The
+// phase parts are reduced modulo one revolution in FP64; a thread's phase
+// base is row + column, its bin and projection bases row + j0 eta and
+// row + j0 ty, formed in FP32 from the record (eta = e32 / 32 exactly).
+constexpr int kBaseEntries = kWarps + 32 / 4;
 
 // Records (and base tables when base_s != nullptr) and window copies of
 // stage b into one buffer.  Warp w produces slots w, w + 8, ...: lane 0
@@ -235,6 +236,43 @@ __device__ __forceinline__ void prefetch_records(const BpLaunch &L, const PulseG
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
+// Base tables of one (tile, pulse) from its record's FP64 steps (every lane
+// of the warp writes its column entry, lanes 0..7 the row entries; the row
+// entries carry -kr in their fourth word, so the forward kernel's
+// consumers read it with the row part).
+__device__ __forceinline__ void write_base_table(float4 *tab, int lane, int tx_half, int W, double A, double alpha,
+                                                 double beta, double B0, double gam, float tx, float kr) {
+    const int j0 = lane - kTY / 2;
+    const double pc = static_cast<double>(j0) * beta;
+    reinterpret_cast<float *>(tab + kWarps)[lane] = static_cast<float>(kTwoPi * (pc - rint(pc)));
+    if (lane < kWarps) {
+        const int i0 = lane - tx_half;
+        const double pr = fma(static_cast<double>(i0), alpha, A);
+        tab[lane] = make_float4(static_cast<float>(kTwoPi * (pr - rint(pr))),
+                                static_cast<float>(fma(static_cast<double>(i0), gam, B0 - W)),
+                                static_cast<float>(i0) * tx, -kr);
+    }
+}
+
+// Lane 0: the window copy of pulse p (slot q) into the stage buffer, or a
+// plain arrival when the tile's window misses the pulse's range bins.
+__device__ __forceinline__ void issue_window(const BpLaunch &L, int p, int q, int flags, int wp, int ws,
+                                             uint32_t win_s, uint32_t bar) {
+    if (flags & PG_ACTIVE) {
+        // the pulse's tight window, at its place inside the slot's full one
+        const int off = L.W - wp;
+        const uint32_t bytes = static_cast<uint32_t>(2 * wp + 2) * 16u;
+        const float4 *src =
+            static_cast<const float4 *>(L.pairs) + static_cast<long long>(p) * L.row_stride + L.guard + ws + off;
+        mbar_arrive_expect_tx(bar, bytes);
+        bulk_copy_g2s(win_s + (static_cast<uint32_t>(q) * static_cast<uint32_t>(L.wsize) + static_cast<uint32_t>(off)) *
+                                  16u,
+                      src, bytes, bar);
+    } else {
+        mbar_arrive(bar);
+    }
+}
+
 // Records, base tables and window copies of stage b (see below).  stg: the
 // stage's prefetched records (prefetch_records), or nullptr: lane 0 computes
 // them (make_geo).
@@ -246,46 +284,55 @@ __device__ __forceinline__ void produce_slots(const BpLaunch &L, int b, PulseGeo
     if (stg) {
         asm volatile("cp.async.wait_all;" ::: "memory");
         __syncwarp();
+        for (int q = warp; q < PB; q += kWarps) {
+            const int p = b * PB + q;
+            const bool valid = p < L.np;
+            // lanes 0..7 move the record's 16-byte words into the stage's
+            // record slot (zeros past the last pulse: flags 0); every lane
+            // reads the steps of the tables itself (broadcast loads)
+            const float4 *rec = reinterpret_cast<const float4 *>(stg + q);
+            if (lane < 8)
+                reinterpret_cast<float4 *>(geo_s + q)[lane] = valid ? rec[lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+            if (base_s) {
+                double2 d0 = make_double2(0.0, 0.0), d1 = d0;
+                double gam = 0.0;
+                float tx = 0.0f, kr = 0.0f;
+                if (valid) {
+                    const double2 *rd = reinterpret_cast<const double2 *>(stg + q);
+                    d0 = rd[0];  // A, alpha
+                    d1 = rd[1];  // beta, B0
+                    gam = stg[q].gam;
+                    tx = stg[q].tx;
+                    kr = stg[q].kr;
+                }
+                write_base_table(base_s + q * kBaseEntries, lane, tx_half, L.W, d0.x, d0.y, d1.x, d1.y, gam, tx, kr);
+            }
+            __syncwarp();
+            if (lane == 0 && valid) {
+                const int4 f = *reinterpret_cast<const int4 *>(&stg[q].ws);  // ws, flags, wp, pad
+                issue_window(L, p, q, f.y, f.z, f.x, win_s, bar);
+            } else if (lane == 0) {
+                mbar_arrive(bar);
+            }
+        }
+        return;
     }
     for (int q = warp; q < PB; q += kWarps) {
         const int p = b * PB + q;
         PulseGeo g = {};
-        if (lane == 0 && p < L.np) g = stg ? stg[q] : make_geo(L, p, goff, cx, cy, cz, tx_half);
+        if (lane == 0 && p < L.np) g = make_geo(L, p, goff, cx, cy, cz, tx_half);
         if (base_s) {
             const unsigned full = 0xffffffffu;
             const double A = __shfl_sync(full, g.A, 0), alpha = __shfl_sync(full, g.alpha, 0);
             const double beta = __shfl_sync(full, g.beta, 0), B0 = __shfl_sync(full, g.B0, 0);
-            const double gam = __shfl_sync(full, g.gam, 0), eta = __shfl_sync(full, g.eta, 0);
-            const float tx = __shfl_sync(full, g.tx, 0), ty = __shfl_sync(full, g.ty, 0);
-            float4 *tab = base_s + q * kBaseEntries;
-            const int j0 = lane - kTY / 2;
-            const double pc = static_cast<double>(j0) * beta;
-            tab[lane] = make_float4(static_cast<float>(kTwoPi * (pc - rint(pc))), static_cast<float>(j0 * eta),
-                                    static_cast<float>(j0) * ty, 0.0f);
-            if (lane < kWarps) {
-                const int i0 = lane - tx_half;
-                const double pr = fma(static_cast<double>(i0), alpha, A);
-                tab[32 + lane] = make_float4(static_cast<float>(kTwoPi * (pr - rint(pr))),
-                                             static_cast<float>(fma(static_cast<double>(i0), gam, B0 - L.W)),
-                                             static_cast<float>(i0) * tx, 0.0f);
-            }
+            const double gam = __shfl_sync(full, g.gam, 0);
+            const float tx = __shfl_sync(full, g.tx, 0), kr = __shfl_sync(full, g.kr, 0);
+            write_base_table(base_s + q * kBaseEntries, lane, tx_half, L.W, A, alpha, beta, B0, gam, tx, kr);
             __syncwarp();
         }
         if (lane != 0) continue;
         geo_s[q] = g;
-        if (g.flags & PG_ACTIVE) {
-            // the pulse's tight window, at its place inside the slot's full one
-            const int off = L.W - g.wp;
-            const uint32_t bytes = static_cast<uint32_t>(2 * g.wp + 2) * 16u;
-            const float4 *src = static_cast<const float4 *>(L.pairs) + static_cast<long long>(p) * L.row_stride +
-                                L.guard + g.ws + off;
-            mbar_arrive_expect_tx(bar, bytes);
-            bulk_copy_g2s(win_s + (static_cast<uint32_t>(q) * static_cast<uint32_t>(L.wsize) +
-                                   static_cast<uint32_t>(off)) * 16u,
-                          src, bytes, bar);
-        } else {
-            mbar_arrive(bar);
-        }
+        issue_window(L, p, q, g.flags, g.wp, g.ws, win_s, bar);
     }
 }
 
