@@ -12,8 +12,13 @@
 // Design (one CTA = one pixel tile of (8*MX) x 64 pixels of one z-slice,
 // 256 threads = 8 warps, each thread MX rows (8 apart) x 2 columns (lane and
 // lane + 32, so the lanes of one gather are one column apart):
-//  * pulses go through shared memory in stages of PB pulses, two stages, one
-//    mbarrier per stage with PB arrivals.  For each pulse slot of the next
+//  * pulses go through shared memory in stages of PB pulses, two stage
+//    buffers, each with three mbarriers: "full" (PB arrivals and the window
+//    bytes), "ready" (all 8 warps have put their windows into intercept
+//    form) and "empty" (all 8 warps have consumed the stage).  A warp waits
+//    only for the buffer it touches next, so the warps of a CTA drift up to
+//    a stage apart instead of meeting at a CTA barrier every stage (1.72 vs
+//    1.76 ms on the large workload, same image).  For each pulse slot of the next
 //    stage one warp (slot mod 8) computes the (tile, pulse) geometry record in
 //    FP64 (tile-centre range, unit vector, phase and bin steps reduced mod 1)
 //    and issues one cp.async.bulk copy of the pulse's range-bin window (the
@@ -58,11 +63,15 @@ constexpr int kCtasPerSm = SARBP_CTAS_PER_SM;
 
 constexpr int kTabEntries = kBaseEntries;
 
-// Dynamic shared memory of the forward kernel: barriers and the zero entry,
-// two stage buffers of PB records, base tables and windows, and two
-// staging slots of PB pre-pass records.
+// Header of the shared memory: six mbarriers (full, ready and empty, two
+// buffers each) and the zero entry.
+constexpr int kHdr = 64;
+
+// Dynamic shared memory of the forward kernel: the header, two stage
+// buffers of PB records, base tables and windows, and two staging slots of
+// PB pre-pass records.
 __host__ __device__ constexpr size_t smem_bytes_of(int pb, int wsize) {
-    return 32 + 2 * static_cast<size_t>(pb) * (sizeof(PulseGeo) + kTabEntries * sizeof(float4)) +
+    return kHdr + 2 * static_cast<size_t>(pb) * (sizeof(PulseGeo) + kTabEntries * sizeof(float4)) +
            2 * static_cast<size_t>(pb) * static_cast<size_t>(wsize) * 16 +
            2 * static_cast<size_t>(pb) * sizeof(PulseGeo);
 }
@@ -286,10 +295,10 @@ __global__ void __launch_bounds__(kThreads, MINB)
     constexpr int TX = 8 * MX;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-    float4 *zero = reinterpret_cast<float4 *>(smem + 16);
-    PulseGeo *geo = reinterpret_cast<PulseGeo *>(smem + 32);
-    float4 *bases = reinterpret_cast<float4 *>(smem + 32 + 2 * PB * sizeof(PulseGeo));
-    const uint32_t win_addr = smem_addr(smem + 32 + 2 * PB * (sizeof(PulseGeo) + kTabEntries * sizeof(float4)));
+    float4 *zero = reinterpret_cast<float4 *>(smem + kHdr - 16);
+    PulseGeo *geo = reinterpret_cast<PulseGeo *>(smem + kHdr);
+    float4 *bases = reinterpret_cast<float4 *>(smem + kHdr + 2 * PB * sizeof(PulseGeo));
+    const uint32_t win_addr = smem_addr(smem + kHdr + 2 * PB * (sizeof(PulseGeo) + kTabEntries * sizeof(float4)));
     const uint32_t zero_addr = smem_addr(zero);
     const uint32_t buf_bytes = static_cast<uint32_t>(PB) * static_cast<uint32_t>(L0.wsize) * 16u;
 
@@ -348,10 +357,18 @@ __global__ void __launch_bounds__(kThreads, MINB)
 #pragma unroll
         for (int l = 0; l < 2; ++l) acc_re[k][l] = acc_im[k][l] = 0.0f;
 
-    const uint32_t bar_base = smem_addr(&bars[0]);  // buffer s barrier at bar_base + 8*s
+    // buffer s: full (windows landed) at bar_base + 8 s, ready at
+    // bar_base + 16 + 8 s, empty at bar_base + 32 + 8 s
+    const uint32_t bar_base = smem_addr(&bars[0]);
+    auto ready_bar = [&](int b) { return bar_base + 16u + 8u * b; };
+    auto empty_bar = [&](int b) { return bar_base + 32u + 8u * b; };
     if (threadIdx.x == 0) {
         mbar_init(bar_base, PB);
         mbar_init(bar_base + 8, PB);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(ready_bar(b), kWarps);
+            mbar_init(empty_bar(b), kWarps);
+        }
         *zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         fence_mbar_init();
     }
@@ -406,15 +423,21 @@ __global__ void __launch_bounds__(kThreads, MINB)
         produce(0, nullptr);
     }
     intercept_slots<PB>(geo, win_addr, bar_base, 0, pc.L->wsize, pc.L->W, warp, lane, pc.L->err);
-    __syncthreads();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(ready_bar(0));
 
     int last_issued = 0;
     int seg = 0;                 // segments flushed so far
     int seg_first = cc.u.b;      // first stage of the open segment
     for (int i = 0; i < n; ++i) {
         const int s = i & 1;
+        bool ok = true;
         if (i + 1 < n) {
             pc.advance(scenes, nscenes, rot_later);
+            // buffer s ^ 1 last held stage i - 1: every warp has consumed it
+            if (i >= 1) ok = mbar_wait_bounded(empty_bar(s ^ 1), ((i - 1) >> 1) & 1, pc.L->err);
+        }
+        if (i + 1 < n && ok) {
             if (pregeo) {
                 // stage i + 1's records were prefetched into staging slot
                 // (i + 1) & 1; stage i + 2's go to the other one, whose
@@ -429,7 +452,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
         const BpLaunch &L = *cc.L;
         const int S = cc.g.stages;
         const int b = cc.u.b;  // position in the tile's stage order
-        const bool ok = mbar_wait_bounded(bar_base + 8 * s, (i >> 1) & 1, L.err);
+        if (ok) ok = mbar_wait_bounded(ready_bar(s), (i >> 1) & 1, L.err);
         if (ok) {
             const int nq = min(PB, L.np - cc.stage() * PB);
             // stage summary: all PB pulses active, none gated or near-field
@@ -465,16 +488,22 @@ __global__ void __launch_bounds__(kThreads, MINB)
                 }
             }
         }
-        // the next stage's windows into intercept form, published by the barrier
-        if (i + 1 < n)
-            intercept_slots<PB>(geo + (s ^ 1) * PB, win_addr + (s ^ 1) * buf_bytes, bar_base + 8 * (s ^ 1),
-                                ((i + 1) >> 1) & 1, pc.L->wsize, pc.L->W, warp, lane, L.err);
-        if (__syncthreads_or(!ok)) {
-            // let the copies already issued for the other buffer (and the
-            // record prefetches) land before the CTA's shared memory goes
-            // away (again bounded)
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty_bar(s));
+        // the next stage's windows into intercept form, published by the
+        // ready mbarrier
+        if (i + 1 < n && ok) {
+            ok = intercept_slots<PB>(geo + (s ^ 1) * PB, win_addr + (s ^ 1) * buf_bytes, bar_base + 8 * (s ^ 1),
+                                     ((i + 1) >> 1) & 1, pc.L->wsize, pc.L->W, warp, lane, L.err);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(ready_bar(s ^ 1));
+        }
+        // a wait ran out (error bit set): this warp stops, the others at
+        // their next wait for it; its own copies and record prefetches land
+        // before the CTA's shared memory goes away (again bounded)
+        if (__any_sync(0xffffffffu, !ok)) {
             asm volatile("cp.async.wait_all;" ::: "memory");
-            if (threadIdx.x == 0 && last_issued > i)
+            if (lane == 0 && last_issued > i)
                 mbar_wait_bounded(bar_base + 8 * (last_issued & 1), (last_issued >> 1) & 1, L.err);
             return;
         }
@@ -483,9 +512,10 @@ __global__ void __launch_bounds__(kThreads, MINB)
             if (seg_first == 0 && b == S - 1) {
                 store_pixels<MX>(L, cc.u.tx * TX, cc.u.ty * kTY, cc.u.hyp * L.nz + cc.u.iz, warp, lane, acc_re,
                                  acc_im);
+                // completion time: the latest of the warps' stores
                 if (BATCH && done) {
-                    __syncthreads();
-                    if (threadIdx.x == 0) atomicMax(done + cc.scene, global_timer_ns());
+                    __syncwarp();
+                    if (lane == 0) atomicMax(done + cc.scene, global_timer_ns());
                 }
             } else {
                 float4 *slot = static_cast<float4 *>(L0.sk_partial) +

@@ -361,10 +361,10 @@ __device__ __forceinline__ float2 splat(float a) { return make_float2(a, a); }
 // the error bit and leaves the windows as they are).  The CTA barrier that
 // follows publishes them.
 template <int PB>
-__device__ __forceinline__ void intercept_slots(const PulseGeo *geo_s, uint32_t win_s, uint32_t bar, uint32_t parity,
+__device__ __forceinline__ bool intercept_slots(const PulseGeo *geo_s, uint32_t win_s, uint32_t bar, uint32_t parity,
                                                 int wsize, int W, int warp, int lane, unsigned *err) {
-    if (warp >= PB) return;
-    if (!mbar_wait_bounded(bar, parity, err)) return;
+    if (warp >= PB) return true;
+    if (!mbar_wait_bounded(bar, parity, err)) return false;
     for (int q = warp; q < PB; q += kWarps) {
         if (!(geo_s[q].flags & PG_ACTIVE)) continue;
         const uint32_t w = win_s + static_cast<uint32_t>(q) * static_cast<uint32_t>(wsize) * 16u;
@@ -380,6 +380,7 @@ __device__ __forceinline__ void intercept_slots(const PulseGeo *geo_s, uint32_t 
     // these generic-proxy stores precede the next bulk copy (async proxy) into
     // the same buffer, issued after the CTA barrier
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    return true;
 }
 
 }  // namespace tile
