@@ -186,8 +186,9 @@ __global__ void __launch_bounds__(kThreads, 2)
     PulseGeo *geo = reinterpret_cast<PulseGeo *>(smem + 32);
     float4 *bases = reinterpret_cast<float4 *>(smem + 32 + 2 * PB * sizeof(PulseGeo));
     float *red = reinterpret_cast<float *>(smem + 32 + 2 * PB * (sizeof(PulseGeo) + kBaseEntries * sizeof(float4)));
-    const uint32_t win_addr = smem_addr(smem + 32 + 2 * PB * (sizeof(PulseGeo) + kBaseEntries * sizeof(float4)) +
-                                        2 * kWarps * 4 * PB * sizeof(float));
+    unsigned char *win_ptr = smem + 32 + 2 * PB * (sizeof(PulseGeo) + kBaseEntries * sizeof(float4)) +
+                             2 * kWarps * 4 * PB * sizeof(float);
+    const uint32_t win_addr = smem_addr(win_ptr);
     const uint32_t zero_addr = smem_addr(zero);
     const int wsize = L.wsize;
     const uint32_t pulse_bytes = static_cast<uint32_t>(wsize) * 16u;
@@ -250,6 +251,16 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
     __syncthreads();
 
+    // Pre-pass records (BpLaunch::geo_tab, [tile][pulse]): the producing
+    // warps copy them from a staging ring filled a stage ahead, after the
+    // two stage buffers' windows.
+    const bool pregeo = L.geo_tab != nullptr;
+    PulseGeo *stg = reinterpret_cast<PulseGeo *>(win_ptr + 2 * buf_bytes);
+    auto prefetch = [&](const UnitCursor &u, int slot) {
+        const long long t = ((static_cast<long long>(u.hyp) * L.nz + u.iz) * tg.tiles_x + u.tx) * tg.tiles_y + u.ty;
+        prefetch_records<PB>(L, static_cast<const PulseGeo *>(L.geo_tab) + t * L.np, u.b, stg + slot * PB, warp,
+                             lane);
+    };
     // records, base tables and windows of the producer cursor's unit into
     // buffer s (every lane of the warp enters produce_slots)
     auto produce = [&](int s) {
@@ -257,8 +268,16 @@ __global__ void __launch_bounds__(kThreads, 2)
         const double cy = L.bottom + static_cast<double>(pc.ty * kTY + kTY / 2) * L.dy;
         const double cz = L.zlow + static_cast<double>(pc.iz) * L.dz;
         produce_slots<PB>(L, pc.b, geo + s * PB, bases + s * PB * kBaseEntries, win_addr + s * buf_bytes,
-                          bar_base + 8 * s, warp, lane, TX / 2, cx, cy, cz);
+                          bar_base + 8 * s, warp, lane, TX / 2, cx, cy, cz, 0, pregeo ? stg + s * PB : nullptr);
     };
+    if (pregeo) {
+        prefetch(pc, 0);
+        if (n > 1) {
+            UnitCursor nx = pc;
+            nx.advance(tg, L);
+            prefetch(nx, 1);
+        }
+    }
     produce(0);
     intercept_slots<PB>(geo, win_addr, bar_base, 0, L.wsize, L.W, warp, lane, L.err);
     __syncthreads();
@@ -270,6 +289,13 @@ __global__ void __launch_bounds__(kThreads, 2)
             pc.advance(tg, L);
             produce(s ^ 1);
             last_issued = i + 1;
+            // stage i + 2's records into the staging slot stage i's producer
+            // read before the last barrier
+            if (pregeo && i + 2 < n) {
+                UnitCursor nx = pc;
+                nx.advance(tg, L);
+                prefetch(nx, s);
+            }
         }
         const int b = cc.b;
         const bool ok = mbar_wait_bounded(bar_base + 8 * s, (i >> 1) & 1, L.err);
@@ -357,8 +383,10 @@ __global__ void __launch_bounds__(kThreads, 2)
             intercept_slots<PB>(geo + (s ^ 1) * PB, win_addr + (s ^ 1) * buf_bytes, bar_base + 8 * (s ^ 1),
                                 ((i + 1) >> 1) & 1, wsize, L.W, warp, lane, L.err);
         if (__syncthreads_or(!ok)) {
-            // let the copies already issued for the other buffer land before
-            // the CTA's shared memory goes away (again bounded)
+            // let the copies already issued for the other buffer (and the
+            // record prefetches) land before the CTA's shared memory goes
+            // away (again bounded)
+            asm volatile("cp.async.wait_all;" ::: "memory");
             if (threadIdx.x == 0 && last_issued > i)
                 mbar_wait_bounded(bar_base + 8 * (last_issued & 1), (last_issued >> 1) & 1, L.err);
             return;
@@ -460,7 +488,14 @@ cudaError_t launch_adj(const BpLaunch &L, const void *grad, void *partials, size
     const long long units = tile_grid(L, TX, PB).units;
     const long long ctas = std::min<long long>(units, static_cast<long long>(sms) * occ);
     if (ctas < 1 || ctas > 0x7fffffffLL) return cudaErrorInvalidValue;
-    kern<<<static_cast<unsigned>(ctas), kThreads, smem, s>>>(L, static_cast<const float2 *>(grad),
+    // the (tile, pulse) records from the pre-pass when the plan holds room
+    // for them, else computed by the producing lanes
+    BpLaunch La = L;
+    bool pregeo = false;
+    e = launch_geo_records(La, MX, &pregeo, s);
+    if (e != cudaSuccess) return e;
+    if (!pregeo) La.geo_tab = nullptr;
+    kern<<<static_cast<unsigned>(ctas), kThreads, smem, s>>>(La, static_cast<const float2 *>(grad),
                                                               static_cast<float4 *>(partials));
     return cudaGetLastError();
 }
@@ -475,7 +510,7 @@ long long bp_tile_count(const BpLaunch &L, const TileConfig &tc) {
 size_t bp_adjoint_smem_bytes(const TileConfig &tc, int wsize) {
     const size_t pb = static_cast<size_t>(tc.pb);
     return 32 + 2 * pb * (sizeof(PulseGeo) + kBaseEntries * sizeof(float4)) + 2 * kWarps * 4 * pb * sizeof(float) +
-           2 * pb * static_cast<size_t>(wsize) * 16;
+           2 * pb * static_cast<size_t>(wsize) * 16 + 2 * pb * sizeof(PulseGeo);
 }
 
 cudaError_t launch_bp_adjoint(const BpLaunch &L, const void *grad, void *partials, const TileConfig &tc, size_t smem,

@@ -595,37 +595,73 @@ __global__ void __launch_bounds__(kThreads)
 
 // Geometry records of every (tile, pulse) of a launch, [tile][pulse], one
 // thread each (make_geo, full warps), for the forward kernel's producers to
-// load.
-// Each CTA computes 256 records into shared memory, then writes them out as
-// consecutive 16-byte words (a warp stores 512 contiguous bytes), not as
-// 128-byte structures 128 bytes apart per lane.
+// load.  Each CTA computes 256 records into shared memory, then writes them
+// out as consecutive 16-byte words (a warp stores 512 contiguous bytes).  In
+// shared memory word k of record r sits at [k][r] with a row stride of 257
+// words, so both the record-per-thread stores and the word-per-thread reads
+// hit 8 distinct bank groups per quarter warp (a [r][k] layout put all 32
+// lanes of each 16-byte store on the same four banks).  Indexes are 32-bit:
+// the launch checks n < 2^31.
 template <int MX>
-__global__ void __launch_bounds__(256) bp_geo_records_kernel(const __grid_constant__ BpLaunch L, long long n) {
+__global__ void __launch_bounds__(256) bp_geo_records_kernel(const __grid_constant__ BpLaunch L, int n) {
     constexpr int TX = 8 * MX;
     constexpr int kWords = sizeof(PulseGeo) / sizeof(float4);
-    __shared__ PulseGeo recs[256];
+    constexpr int kStride = 257;
+    __shared__ float4 words[kWords * kStride];
     const TileGrid tg = tile_grid(L, TX, 1);
+    const unsigned np = static_cast<unsigned>(L.np), ty_n = static_cast<unsigned>(tg.tiles_y),
+                   tx_n = static_cast<unsigned>(tg.tiles_x), nz = static_cast<unsigned>(L.nz);
     float4 *out = static_cast<float4 *>(L.geo_tab);
-    for (long long i0 = blockIdx.x * 256ll; i0 < n; i0 += static_cast<long long>(gridDim.x) * 256) {
-        const long long i = i0 + threadIdx.x;
-        if (i < n) {
-            const long long t = i / L.np;
-            const int p = static_cast<int>(i - t * L.np);
-            int tx0, ty0, zz;
-            tile_origin(tg, t, TX, tx0, ty0, zz);
-            const int hyp = zz / L.nz, iz = zz - hyp * L.nz;
-            const double cx = L.left + static_cast<double>(tx0 + TX / 2) * L.dx;
-            const double cy = L.bottom + static_cast<double>(ty0 + kTY / 2) * L.dy;
+    for (unsigned i0 = blockIdx.x * 256u; i0 < static_cast<unsigned>(n); i0 += gridDim.x * 256u) {
+        const unsigned i = i0 + threadIdx.x;
+        if (i < static_cast<unsigned>(n)) {
+            const unsigned t = i / np, p = i - t * np;
+            const unsigned r = t / ty_n, ty = t - r * ty_n;
+            const unsigned zz = r / tx_n, tx = r - zz * tx_n;
+            const unsigned hyp = zz / nz, iz = zz - hyp * nz;
+            const double cx = L.left + static_cast<double>(static_cast<int>(tx) * TX + TX / 2) * L.dx;
+            const double cy = L.bottom + static_cast<double>(static_cast<int>(ty) * kTY + kTY / 2) * L.dy;
             const double cz = L.zlow + static_cast<double>(iz) * L.dz;
-            recs[threadIdx.x] = make_geo(L, p, static_cast<long long>(hyp) * L.np, cx, cy, cz, TX / 2);
+            const PulseGeo g = make_geo(L, static_cast<int>(p), static_cast<long long>(hyp) * L.np, cx, cy, cz, TX / 2);
+            const float4 *gw = reinterpret_cast<const float4 *>(&g);
+#pragma unroll
+            for (int k = 0; k < kWords; ++k) words[k * kStride + threadIdx.x] = gw[k];
         }
         __syncthreads();
-        const long long words = (n - i0 < 256 ? n - i0 : 256) * kWords;
-        const float4 *src = reinterpret_cast<const float4 *>(recs);
-        for (int w = threadIdx.x; w < words; w += 256) out[i0 * kWords + w] = src[w];
+        const unsigned left = static_cast<unsigned>(n) - i0;
+        const int nw = static_cast<int>((left < 256u ? left : 256u) * kWords);
+        for (int w = threadIdx.x; w < nw; w += 256)
+            out[static_cast<long long>(i0) * kWords + w] = words[(w % kWords) * kStride + w / kWords];
         __syncthreads();
     }
 }
+
+template <int MX>
+cudaError_t launch_records_mx(const BpLaunch &L, bool *ran, cudaStream_t s) {
+    *ran = false;
+    const long long nrec = tile_grid(L, 8 * MX, 1).tiles * L.np;
+    if (!L.geo_tab || nrec < 1 || nrec > L.geo_tab_records || nrec >= 0x7fffffffLL) return cudaSuccess;
+    const long long blocks = (nrec + 255) / 256;
+    bp_geo_records_kernel<MX><<<static_cast<unsigned>(blocks < 148 * 64 ? blocks : 148 * 64), 256, 0, s>>>(
+        L, static_cast<int>(nrec));
+    const cudaError_t e = cudaGetLastError();
+    *ran = e == cudaSuccess;
+    return e;
+}
+
+}  // namespace
+
+cudaError_t launch_geo_records(const BpLaunch &L, int mx, bool *ran, cudaStream_t s) {
+    switch (mx) {
+        case 8: return launch_records_mx<8>(L, ran, s);
+        case 4: return launch_records_mx<4>(L, ran, s);
+        case 2: return launch_records_mx<2>(L, ran, s);
+        case 1: return launch_records_mx<1>(L, ran, s);
+        default: *ran = false; return cudaSuccess;
+    }
+}
+
+namespace {
 
 template <int MX, int PB, bool CHECKED, int MINB>
 cudaError_t launch_kernels(const BpLaunch &L0, size_t smem, cudaStream_t s) {
@@ -636,15 +672,10 @@ cudaError_t launch_kernels(const BpLaunch &L0, size_t smem, cudaStream_t s) {
     const TileGrid tg = tile_grid(L0, TX, PB);
     if (tg.units < 1) return cudaSuccess;
     BpLaunch L = L0;
-    const long long nrec = tg.tiles * L.np;
-    if (L.geo_tab && nrec <= L.geo_tab_records) {
-        const long long blocks = (nrec + 255) / 256;
-        bp_geo_records_kernel<MX><<<static_cast<unsigned>(blocks < 148 * 64 ? blocks : 148 * 64), 256, 0, s>>>(L, nrec);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-    } else {
-        L.geo_tab = nullptr;
-    }
+    bool pregeo = false;
+    e = launch_geo_records(L, MX, &pregeo, s);
+    if (e != cudaSuccess) return e;
+    if (!pregeo) L.geo_tab = nullptr;
     // split the units over the resident CTAs unless the tiles fill whole waves
     long long G = tg.tiles;
     if (L.sk_partial && L.sk_resident > 0 && tg.tiles % L.sk_resident != 0) {

@@ -81,6 +81,11 @@ struct TileConfig {
 
 cudaError_t launch_bp_mixed(const BpLaunch &L, const TileConfig &tc, bool checked, size_t smem,
                             cudaStream_t s);
+// Geometry records of every (tile, pulse) of L into L.geo_tab for tiles of
+// (8 mx) x 64 pixels (bp_mixed.cu).  *ran is false (nothing launched) when
+// L.geo_tab is null or holds fewer records than the launch has; the kernels
+// then compute the records themselves.
+cudaError_t launch_geo_records(const BpLaunch &L, int mx, bool *ran, cudaStream_t s);
 cudaError_t launch_bp_fp64(const BpLaunch &L, const TileConfig &tc, size_t smem, cudaStream_t s);
 size_t bp_mixed_smem_bytes(const TileConfig &tc, int wsize);
 // Adjoint (bp_adjoint.cu): per-(tile, pulse) gradient partials, then a sum
