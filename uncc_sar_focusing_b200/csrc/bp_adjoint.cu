@@ -18,7 +18,10 @@
 // nu = kr / lambda and Z = v' + j nu v
 //     s_pq = lambda |G_q| Re(Z exp(j (phi - psi_q))):
 // the conjugate product with G becomes a phase offset folded into the sine /
-// cosine argument, and lambda leaves the pixel loop.  Writing d = (i dx, j dy, 0)
+// cosine argument, and lambda leaves the pixel loop.  The producing warps
+// rewrite each window entry to {v' + j nu c, j nu v'} (the intercept form's
+// c = v_n - (n - W) v'_n), so Z at a pixel's window-centred bin B is one
+// fused multiply-add per component, Z = Zc + B Zv.  Writing d = (i dx, j dy, 0)
 // for a pixel's offset from the tile centre (i, j its row and column offsets)
 // and Rc/R_q = 1 + t_eff/Rc, d/R_q = d_eff/Rc (far field: t_eff = u.d =
 // i ux dx + j uy dy, d_eff = d; near field: the exact ratios),
@@ -56,7 +59,7 @@ template <int MX, bool GATE, bool NEAR>
 __device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, const float4 *base, uint32_t w_addr,
                                               uint32_t zero_addr, int warp, int lane, float lam,
                                               const float2 (&nd2)[MX], const float2 (&npsi)[MX],
-                                              const float2 (&gm)[MX], float i0f, float j0f, float inv_lam, int W,
+                                              const float2 (&gm)[MX], float i0f, float j0f, int W,
                                               float2 &T, float2 &V, float4 &E) {
     const float4 c0 = *reinterpret_cast<const float4 *>(&g.a8r);  // a8r, b32r, g8, e32
     const float4 c1 = *reinterpret_cast<const float4 *>(&g.tx);   // tx, ty, h, hr
@@ -73,7 +76,6 @@ __device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, const float4 *b
     const float2 MAGIC = splat(kRoundMagic);
     // B is the window-centred bin (entry floor(B) + W, intercept form)
     const uint32_t w_adj = w_addr + (static_cast<uint32_t>(W) - kRoundMagicBits) * 16u;
-    const float nu = c2.x * inv_lam;
 #pragma unroll
     for (int k = 0; k < MX; ++k) {
         if (k > 0) {
@@ -110,13 +112,11 @@ __device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, const float4 *b
                 const bool valid = (Bl > c2.z) && (Bl < c2.w);
                 addr = valid ? addr : zero_addr;
             }
-            // intercept-form entry {c, v'}: v(B) = c + B v'
+            // Z-form entry {Zc, Zv}: Z(B) = v' + j nu v(B) = Zc + B Zv;
+            // s~ = Re(Z exp(j theta))
             const float4 v = lds128(addr);
-            const float vr = fmaf(Bl, v.z, v.x);
-            const float vi = fmaf(Bl, v.w, v.y);
-            // Z = v' + j nu v; s~ = Re(Z exp(j theta))
-            const float zr = fmaf(-nu, vi, v.z);
-            const float zi = fmaf(nu, vr, v.w);
+            const float zr = fmaf(Bl, v.z, v.x);
+            const float zi = fmaf(Bl, v.w, v.y);
             const float sl = fmaf(zr, cs, -zi * sn);
             if (l) st.y = sl;
             else st.x = sl;
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
     }
     produce(0);
-    intercept_slots<PB>(geo, win_addr, bar_base, 0, L.wsize, L.W, warp, lane, L.err);
+    intercept_slots<PB, true>(geo, win_addr, bar_base, 0, L.wsize, L.W, warp, lane, L.err, inv_lam);
     __syncthreads();
 
     int last_issued = 0;
@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                     float4 E;
                     adjoint_pulse<MX, false, false>(geo[s * PB + q], bases + (s * PB + q) * kBaseEntries,
                                                     w0 + q * pulse_bytes, zero_addr, warp, lane, lam, nd2, npsi, gm,
-                                                    i0f, j0f, inv_lam, L.W, T, V, E);
+                                                    i0f, j0f, L.W, T, V, E);
                     far_sums(r, T, V);
                 }
             } else if (ok) {
@@ -363,14 +363,14 @@ __global__ void __launch_bounds__(kThreads, 2)
                     float4 E = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                     if (g.flags & PG_NEAR) {
                         adjoint_pulse<MX, true, true>(g, bq, w, zero_addr, warp, lane, lam, nd2, npsi, gm, i0f, j0f,
-                                                      inv_lam, L.W, T, V, E);
+                                                      L.W, T, V, E);
                         v[4 * r + 0] = E.x;
                         v[4 * r + 1] = E.y;
                         v[4 * r + 2] = E.z;
                         v[4 * r + 3] = E.w;
                     } else {
                         adjoint_pulse<MX, true, false>(g, bq, w, zero_addr, warp, lane, lam, nd2, npsi, gm, i0f,
-                                                       j0f, inv_lam, L.W, T, V, E);
+                                                       j0f, L.W, T, V, E);
                         far_sums(r, T, V);
                     }
                 }
@@ -380,8 +380,8 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
         // the next stage's windows into intercept form, published by the barrier
         if (i + 1 < n)
-            intercept_slots<PB>(geo + (s ^ 1) * PB, win_addr + (s ^ 1) * buf_bytes, bar_base + 8 * (s ^ 1),
-                                ((i + 1) >> 1) & 1, wsize, L.W, warp, lane, L.err);
+            intercept_slots<PB, true>(geo + (s ^ 1) * PB, win_addr + (s ^ 1) * buf_bytes, bar_base + 8 * (s ^ 1),
+                                      ((i + 1) >> 1) & 1, wsize, L.W, warp, lane, L.err, inv_lam);
         if (__syncthreads_or(!ok)) {
             // let the copies already issued for the other buffer (and the
             // record prefetches) land before the CTA's shared memory goes

@@ -348,6 +348,10 @@ __device__ __forceinline__ void sts64(uint32_t addr, float x, float y) {
     asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(x), "f"(y) : "memory");
 }
 
+__device__ __forceinline__ void sts128(uint32_t addr, float x, float y, float z, float w) {
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(x), "f"(y), "f"(z), "f"(w) : "memory");
+}
+
 __device__ __forceinline__ float2 splat(float a) { return make_float2(a, a); }
 
 // Intercept form of the windows: entry n of a pulse's window holds
@@ -358,11 +362,17 @@ __device__ __forceinline__ float2 splat(float a) { return make_float2(a, a); }
 // with one fused multiply-add and no fraction.  Warp `warp` rewrites the
 // slots it produced (q = warp, warp + 8, ...) of one stage buffer once their
 // copies have landed (bounded wait on the buffer's mbarrier; a timeout sets
-// the error bit and leaves the windows as they are).  The CTA barrier that
+// the error bit and leaves the windows as they are).  The barrier that
 // follows publishes them.
-template <int PB>
+// ZFORM (the adjoint, which needs only Z(B) = v'(B) + j nu v(B), nu = kr /
+// lambda radians per bin): the entry becomes {Zc, Zv} with Zc = v'_n + j nu
+// c_n and Zv = j nu v'_n, so that Z(B) = Zc + B Zv is again one fused
+// multiply-add per component and the pixel loop neither interpolates v nor
+// forms Z.
+template <int PB, bool ZFORM = false>
 __device__ __forceinline__ bool intercept_slots(const PulseGeo *geo_s, uint32_t win_s, uint32_t bar, uint32_t parity,
-                                                int wsize, int W, int warp, int lane, unsigned *err) {
+                                                int wsize, int W, int warp, int lane, unsigned *err,
+                                                float inv_lam = 0.0f) {
     if (warp >= PB) return true;
     if (!mbar_wait_bounded(bar, parity, err)) return false;
     for (int q = warp; q < PB; q += kWarps) {
@@ -370,11 +380,16 @@ __device__ __forceinline__ bool intercept_slots(const PulseGeo *geo_s, uint32_t 
         const uint32_t w = win_s + static_cast<uint32_t>(q) * static_cast<uint32_t>(wsize) * 16u;
         // the entries the pulse's tight window copied
         const int wp = geo_s[q].wp;
+        const float nu = ZFORM ? geo_s[q].kr * inv_lam : 0.0f;
         for (int n = W - wp + lane; n < W + wp + 2; n += 32) {
             const uint32_t a = w + static_cast<uint32_t>(n) * 16u;
             const float4 e = lds128(a);
             const float m = static_cast<float>(n - W);
-            sts64(a, fmaf(-m, e.z, e.x), fmaf(-m, e.w, e.y));
+            const float cr = fmaf(-m, e.z, e.x), ci = fmaf(-m, e.w, e.y);
+            if (ZFORM)
+                sts128(a, fmaf(-nu, ci, e.z), fmaf(nu, cr, e.w), -nu * e.w, nu * e.z);
+            else
+                sts64(a, cr, ci);
         }
     }
     // these generic-proxy stores precede the next bulk copy (async proxy) into
