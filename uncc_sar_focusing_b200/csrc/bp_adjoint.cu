@@ -99,7 +99,7 @@ __device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, const float4 *b
         const float2 TH = __ffma2_rn(NKR, ng, __fadd2_rn(Pb, npsi[k]));
         const float2 B = __ffma2_rn(NLAM, ng, Bb);
         const float2 y = __fadd2_rd(B, MAGIC);
-        float2 st;  // s~ of the pair
+        float2 ZR, NZI, CS, SN;  // the pair's Re Z, -Im Z and rotations
 #pragma unroll
         for (int l = 0; l < 2; ++l) {
             const float Tl = l ? TH.y : TH.x;
@@ -112,15 +112,24 @@ __device__ __forceinline__ void adjoint_pulse(const PulseGeo &g, const float4 *b
                 const bool valid = (Bl > c2.z) && (Bl < c2.w);
                 addr = valid ? addr : zero_addr;
             }
-            // Z-form entry {Zc, Zv}: Z(B) = v' + j nu v(B) = Zc + B Zv;
-            // s~ = Re(Z exp(j theta))
+            // Z-form entry {Zc, Zv}: Z(B) = v' + j nu v(B) = Zc + B Zv
             const float4 v = lds128(addr);
             const float zr = fmaf(Bl, v.z, v.x);
-            const float zi = fmaf(Bl, v.w, v.y);
-            const float sl = fmaf(zr, cs, -zi * sn);
-            if (l) st.y = sl;
-            else st.x = sl;
+            const float nzi = fmaf(-Bl, v.w, -v.y);
+            if (l) {
+                ZR.y = zr;
+                NZI.y = nzi;
+                CS.y = cs;
+                SN.y = sn;
+            } else {
+                ZR.x = zr;
+                NZI.x = nzi;
+                CS.x = cs;
+                SN.x = sn;
+            }
         }
+        // s~ = Re(Z exp(j theta)) of the pair as paired FP32
+        const float2 st = __ffma2_rn(ZR, CS, __fmul2_rn(NZI, SN));
         if (NEAR) {
             const float2 sh = __fmul2_rn(gm[k], st);
             const float ik = i0f + static_cast<float>(8 * k);
