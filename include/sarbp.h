@@ -341,6 +341,21 @@ SARBP_API int sarbp_plan_check(sarbp_plan *plan, void *stream);
 SARBP_API int sarbp_backproject_noalloc(const sarbp_plan_desc *desc, const void *range_profiles,
                                         const sarbp_geometry *geometry, void *image, int flags, void *stream);
 
+/* ---- test hooks (failure injection; not for production use) ----------- */
+
+/* The device allocation `after` allocations from now (0: the next one) fails
+ * as if the device were out of memory; the hook then disarms itself.
+ * after < 0 disarms it.  Counts the allocations of plans and batches in this
+ * process (cudaMalloc through the library).  Returns SARBP_OK. */
+SARBP_API int sarbp_test_fail_device_alloc(int after);
+
+/* Forward and adjoint kernels of this plan: the producer of pulse `pulse`
+ * expects its range-bin window's bytes but issues no copy, so the pulse's
+ * stage never completes, the kernels' bounded waits run out (about 2 s) and
+ * the call returns SARBP_ERR_KERNEL_TIMEOUT with the device context intact.
+ * pulse < 0 turns it off.  Mixed-precision plans only. */
+SARBP_API int sarbp_test_drop_window_copy(sarbp_plan *plan, int pulse);
+
 #ifdef __cplusplus
 }
 #endif

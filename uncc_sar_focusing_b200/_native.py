@@ -43,6 +43,7 @@ EXPORTED = (
     "sarbp_backproject_adjoint", "sarbp_backproject_hypotheses", "sarbp_focus_submit", "sarbp_focus_wait", "sarbp_plan_get_info",
     "sarbp_batch_create", "sarbp_batch_destroy", "sarbp_batch_focus", "sarbp_batch_wait", "sarbp_batch_autotune",
     "sarbp_batch_get_info", "sarbp_batch_set_schedule", "sarbp_matched_filter", "sarbp_plan_set_range_weights",
+    "sarbp_test_fail_device_alloc", "sarbp_test_drop_window_copy",
 )
 
 
@@ -123,6 +124,8 @@ def lib():
         L.sarbp_batch_set_schedule.argtypes = [vp, i]
         L.sarbp_matched_filter.argtypes = [vp, P(Aperture), vp, i, vp]
         L.sarbp_plan_set_range_weights.argtypes = [vp, vp]
+        L.sarbp_test_fail_device_alloc.argtypes = [i]
+        L.sarbp_test_drop_window_copy.argtypes = [vp, i]
         for name in EXPORTED:
             if name != "sarbp_status_string":
                 getattr(L, name).restype = i

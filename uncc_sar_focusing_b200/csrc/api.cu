@@ -136,7 +136,7 @@ void release(sarbp_plan *p) {
 }
 
 int alloc(sarbp_plan *p, void **ptr, size_t bytes) {
-    const cudaError_t e = cudaMalloc(ptr, bytes);
+    const cudaError_t e = host::device_malloc(ptr, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
         *ptr = nullptr;
@@ -247,6 +247,7 @@ BpLaunch launch_params(const sarbp_plan *p, const double *ax, const double *ay, 
     L.sk_resident = p->sk_resident;
     L.geo_tab = p->d_geotab;
     L.geo_tab_records = p->geotab_records;
+    L.drop_pulse = p->drop_pulse;
     return L;
 }
 
@@ -788,6 +789,19 @@ int sarbp_plan_get_info(const sarbp_plan *plan, sarbp_plan_info *info) {
     info->smem_bytes = static_cast<long long>(plan->smem);
     info->kernels_per_backproject = (plan->d_sk && plan->sk_resident > 0 && info->tiles % plan->sk_resident != 0) ? 2 : 1;
     info->fused_range_compression = plan->d_rctab ? 1 : 0;
+    return SARBP_OK;
+}
+
+int sarbp_test_fail_device_alloc(int after) {
+    host::g_alloc_countdown.store(after < 0 ? -1 : after);
+    return SARBP_OK;
+}
+
+int sarbp_test_drop_window_copy(sarbp_plan *plan, int pulse) {
+    if (!plan) return SARBP_ERR_NULL_POINTER;
+    if (plan->precision != SARBP_PRECISION_MIXED) return SARBP_ERR_UNSUPPORTED;
+    SARBP_TRY(drain_pipe(plan));
+    plan->drop_pulse = pulse < 0 ? -1 : pulse;
     return SARBP_OK;
 }
 

@@ -71,7 +71,7 @@ namespace {
 __global__ void stamp_kernel(unsigned long long *t) { *t = global_timer_ns(); }
 
 int balloc(sarbp_batch *b, void **p, size_t bytes) {
-    const cudaError_t e = cudaMalloc(p, bytes);
+    const cudaError_t e = host::device_malloc(p, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
         *p = nullptr;
@@ -195,6 +195,7 @@ int fill_table(sarbp_batch *b, const sarbp_aperture *aps, void *const *images) {
         BatchScene &T = b->h_table[i];
         std::memset(&T, 0, sizeof(T));
         BpLaunch &L = T.L;
+        L.drop_pulse = -1;
         L.pairs = b->d_pairs[i];
         L.row_stride = b->row_stride[i];
         L.guard = b->guard[i];

@@ -422,9 +422,16 @@ __global__ void __launch_bounds__(kThreads, MINB)
     } else {
         produce(0, nullptr);
     }
-    intercept_slots<PB>(geo, win_addr, bar_base, 0, pc.L->wsize, pc.L->W, warp, lane, pc.L->err);
+    const bool ok0 = intercept_slots<PB>(geo, win_addr, bar_base, 0, pc.L->wsize, pc.L->W, warp, lane, pc.L->err);
     __syncwarp();
     if (lane == 0) mbar_arrive(ready_bar(0));
+    if (__any_sync(0xffffffffu, !ok0)) {
+        // stage 0's copies never completed (error bit set): leave once the
+        // record prefetches have landed; the other warps leave at their next
+        // wait (every arrival on the incomplete barrier's phase is made)
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        return;
+    }
 
     int last_issued = 0;
     int seg = 0;                 // segments flushed so far

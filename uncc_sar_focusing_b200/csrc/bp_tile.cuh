@@ -255,13 +255,18 @@ __device__ __forceinline__ void write_base_table(float4 *tab, int lane, int tx_h
 }
 
 // Lane 0: the window copy of pulse p (slot q) into the stage buffer, or a
-// plain arrival when the tile's window misses the pulse's range bins.
+// plain arrival when the tile's window misses the pulse's range bins.  The
+// test hook L.drop_pulse expects that pulse's bytes without copying them.
 __device__ __forceinline__ void issue_window(const BpLaunch &L, int p, int q, int flags, int wp, int ws,
                                              uint32_t win_s, uint32_t bar) {
     if (flags & PG_ACTIVE) {
         // the pulse's tight window, at its place inside the slot's full one
         const int off = L.W - wp;
         const uint32_t bytes = static_cast<uint32_t>(2 * wp + 2) * 16u;
+        if (p == L.drop_pulse) {
+            mbar_arrive_expect_tx(bar, bytes);
+            return;
+        }
         const float4 *src =
             static_cast<const float4 *>(L.pairs) + static_cast<long long>(p) * L.row_stride + L.guard + ws + off;
         mbar_arrive_expect_tx(bar, bytes);

@@ -3,6 +3,7 @@
 // grid axes, window geometry and the range-compression factors.
 #pragma once
 
+#include <atomic>
 #include <cmath>
 #include <cuda_runtime.h>
 #include <cufft.h>
@@ -19,6 +20,26 @@ inline int from_cuda(cudaError_t e) {
     if (e == cudaErrorMemoryAllocation) return SARBP_ERR_OUT_OF_MEMORY;
     if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return SARBP_ERR_NO_DEVICE;
     return SARBP_ERR_CUDA;
+}
+
+// Failure injection for device allocations (sarbp_test_fail_device_alloc):
+// the number of allocations to let through before one fails, -1: off.
+inline std::atomic<long long> g_alloc_countdown{-1};
+
+// cudaMalloc, or cudaErrorMemoryAllocation (nothing allocated) when the
+// injection countdown reaches this allocation.
+inline cudaError_t device_malloc(void **p, size_t bytes) {
+    long long c = g_alloc_countdown.load();
+    while (c >= 0) {
+        if (g_alloc_countdown.compare_exchange_weak(c, c - 1)) {
+            if (c == 0) {
+                *p = nullptr;
+                return cudaErrorMemoryAllocation;
+            }
+            break;
+        }
+    }
+    return cudaMalloc(p, bytes);
 }
 
 inline int from_cufft(cufftResult r) {

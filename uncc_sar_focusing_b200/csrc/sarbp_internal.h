@@ -43,6 +43,9 @@ struct BpLaunch {
     // records the buffer holds; nullptr: computed in the kernel.
     void *geo_tab;
     long long geo_tab_records;
+    // test hook (sarbp_test_drop_window_copy): the pulse whose window copy the
+    // producers leave out while still expecting its bytes; -1: none
+    int drop_pulse = -1;
 };
 
 // One scene of a batch (sarbp_batch_focus), in device memory.  The forward
@@ -179,6 +182,7 @@ struct sarbp_plan {
     void *d_sk;       // partial sums of tiles split over CTAs (BpLaunch::sk_partial)
     size_t sk_bytes;
     int sk_resident;  // resident CTAs of the plan's forward kernel
+    int drop_pulse = -1;  // test hook: BpLaunch::drop_pulse of the plan's launches
     size_t bytes;     // device bytes held
     cufftHandle fft;
     bool fft_ok;
