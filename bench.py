@@ -74,6 +74,8 @@ def parse_args():
                     help="one warm-up and one focus step of the workload, then two adjoint calls (mixed), "
                          "nothing else (for ncu captures)")
     ap.add_argument("--pulses", type=int, default=0, help="use only the first N pulses (profiling)")
+    ap.add_argument("--log", default="", help="append the result with the run's host, GPU and seed to this "
+                                               "JSON-lines file")
     ap.add_argument("--profile-reference", action="store_true",
                     help="the reference's own GPU kernels on the workload, one untimed and one timed run, "
                          "nothing else (for ncu captures)")
@@ -275,6 +277,8 @@ def reference_arm(args):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if not args.no_reference_gpu:
         line["reference_gpu"] = reference_gpu_rate(sc)
+    if args.log:
+        append_run_log(args.log, line, sc.seed)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -566,6 +570,40 @@ def volumetric_section(dev, steps: int):
     }
 
 
+def append_run_log(path: str, line: dict, seed: int) -> None:
+    """One JSON line per run: the result line, the scene seed, the command,
+    and the host and GPU it ran on (CPU model and cores, GPU name, SMs,
+    memory, compute capability, driver, CUDA and torch versions)."""
+    import platform
+
+    import torch
+
+    cpu = platform.processor() or ""
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for row in fh:
+                if row.startswith("model name"):
+                    cpu = row.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    gpu = {}
+    if torch.cuda.is_available():
+        prop = torch.cuda.get_device_properties(torch.cuda.current_device())
+        gpu = {"name": prop.name, "sms": prop.multi_processor_count, "memory_gib": prop.total_memory / 2**30,
+               "cc": f"{prop.major}.{prop.minor}", "cuda": torch.version.cuda}
+        try:
+            out = subprocess.run(["nvidia-smi", "--query-gpu=driver_version", "--format=csv,noheader"],
+                                 capture_output=True, text=True, timeout=20)
+            gpu["driver"] = out.stdout.strip().splitlines()[0] if out.returncode == 0 and out.stdout else None
+        except Exception:
+            gpu["driver"] = None
+    rec = {"time": time.strftime("%Y-%m-%dT%H:%M:%S%z"), "argv": sys.argv[1:], "scene_seed": seed,
+           "host": {"cpu": cpu, "cores": os.cpu_count()}, "gpu": gpu, "torch": torch.__version__, "result": line}
+    with open(path, "a") as fh:
+        fh.write(json.dumps(rec) + "\n")
+
+
 def profiled_traffic(config: str):
     """DRAM bytes per backprojection launch from the committed ncu summary of
     this workload (profiles/), or None."""
@@ -835,6 +873,8 @@ def gpu_arm(args):
         dist.barrier()
         dist.destroy_process_group()
     if line is not None:
+        if args.log:
+            append_run_log(args.log, line, sc.seed)
         print(json.dumps(line), flush=True)
     return 0
 

@@ -196,3 +196,15 @@ def test_reference_dft_costs_batch_equals_single():
     batch = AF.reference_dft_costs(imgs)
     for i in range(4):
         assert abs(float(batch[i]) - AF.reference_dft_cost(imgs[i])) < 1e-9 * abs(float(batch[i]))
+
+
+def test_autofocus_state_round_trips_through_npz(tmp_path):
+    rng = np.random.default_rng(3)
+    st = AF.AutofocusState(theta=rng.standard_normal((3, 4)), exp_avg=rng.standard_normal((3, 4)),
+                           exp_avg_sq=rng.random((3, 4)), step=17.0, iters_done=17, total_iters=300, lr=0.02)
+    path = str(tmp_path / "state.npz")
+    st.save(path)
+    back = AF.AutofocusState.load(path)
+    for name in ("theta", "exp_avg", "exp_avg_sq"):
+        assert np.array_equal(getattr(back, name), getattr(st, name))
+    assert (back.step, back.iters_done, back.total_iters, back.lr) == (17.0, 17, 300, 0.02)

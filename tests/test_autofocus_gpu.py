@@ -93,6 +93,37 @@ def test_captured_descent_matches_eager(torch_cuda):
         assert torch.allclose(rg, re_, rtol=0, atol=1e-9)
 
 
+def test_gradient_autofocus_resumes_from_a_saved_state(torch_cuda, tmp_path):
+    """A descent split in two, the first part's state written to .npz and
+    read back for the second, reaches the coefficients and Adam moments of
+    the whole run (same schedule positions, same optimiser state)."""
+    torch = torch_cuda
+    from uncc_sar_focusing_b200 import autofocus as AF
+    from uncc_sar_focusing_b200 import focusing
+
+    sc = S.motion_error_scene(K=128, Np=256, n=128, spacing=0.16, peak=0.3, walk_sigma=5e-4, seed=11,
+                              device="cuda")
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    ax, ay, az, r0, f0 = (dev(v) for v in (sc.ant_x, sc.ant_y, sc.ant_z, sc.slant_range, sc.start_freq))
+    with focusing.Plan.for_scene(sc, "mixed") as plan:
+        plan.range_compress(dev(sc.phase_history))
+        motion = AF.CubicMotion(ax, ay, az)
+        whole = AF.gradient_autofocus(plan, motion, r0, f0, iters=30, graph=False)
+        first = AF.gradient_autofocus(plan, motion, r0, f0, iters=12, total_iters=30, graph=False)
+        first.state.save(str(tmp_path / "autofocus.npz"))
+        state = AF.AutofocusState.load(str(tmp_path / "autofocus.npz"))
+        assert state.iters_done == 12 and state.total_iters == 30
+        second = AF.gradient_autofocus(plan, motion, r0, f0, iters=18, resume=state, graph=False)
+    assert second.history[0]["iter"] == 12 and second.state.iters_done == 30
+    assert second.state.step == whole.state.step == 30
+    for name in ("theta", "exp_avg", "exp_avg_sq"):
+        a, b = getattr(second.state, name), getattr(whole.state, name)
+        assert np.allclose(a, b, rtol=1e-12, atol=0), (name, np.abs(a - b).max())
+    # the entropies of the second part are the whole run's last 18
+    assert np.allclose([h["entropy"] for h in second.history], [h["entropy"] for h in whole.history[12:]],
+                       rtol=1e-12, atol=0)
+
+
 def test_reference_costs_on_the_gpu_match_the_transcriptions(torch_cuda):
     """The reference's two grid-search costs, batched on the device, against
     direct transcriptions of the reference's loops (dft2DCalculation,

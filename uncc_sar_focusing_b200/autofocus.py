@@ -176,33 +176,87 @@ def _descend(step, iters: int, lr_at, lr: torch.Tensor, record, graph: bool, war
 
 
 @dataclasses.dataclass
+class AutofocusState:
+    """Where a gradient autofocus run stopped: the last iterate of the 12
+    coefficients, Adam's moments and step count, and the schedule position
+    (`iters_done` of `total_iters` steps), enough to resume it exactly."""
+
+    theta: np.ndarray       # [3, 4] float64
+    exp_avg: np.ndarray     # [3, 4] Adam first moment
+    exp_avg_sq: np.ndarray  # [3, 4] Adam second moment
+    step: float             # Adam step count
+    iters_done: int
+    total_iters: int
+    lr: float
+
+    def save(self, path: str) -> None:
+        """Write the state to an .npz file."""
+        np.savez(path, theta=self.theta, exp_avg=self.exp_avg, exp_avg_sq=self.exp_avg_sq,
+                 step=np.float64(self.step), iters_done=np.int64(self.iters_done),
+                 total_iters=np.int64(self.total_iters), lr=np.float64(self.lr))
+
+    @classmethod
+    def load(cls, path: str) -> "AutofocusState":
+        with np.load(path) as z:
+            return cls(theta=z["theta"].copy(), exp_avg=z["exp_avg"].copy(), exp_avg_sq=z["exp_avg_sq"].copy(),
+                       step=float(z["step"]), iters_done=int(z["iters_done"]), total_iters=int(z["total_iters"]),
+                       lr=float(z["lr"]))
+
+
+@dataclasses.dataclass
 class AutofocusResult:
 
     theta: torch.Tensor
     history: List[dict]
     seconds: float
     images_formed: int
+    state: Optional[AutofocusState] = None  # the last iterate, to resume from
 
 
 def gradient_autofocus(plan: Plan, motion: CubicMotion, slant_range, start_freq, iters: int = 200,
                        lr: float = 0.02, theta0: Optional[torch.Tensor] = None, coarse_to_fine: bool = True,
-                       log_every: int = 1, graph: bool = True) -> AutofocusResult:
+                       log_every: int = 1, graph: bool = True, resume: Optional[AutofocusState] = None,
+                       total_iters: Optional[int] = None) -> AutofocusResult:
     """Adam on the 12 coefficients, loss = image entropy, gradient through the
     adjoint backprojection.  With coarse_to_fine the step size decays from
     `lr` metres to lr/100 (cosine, as CosineAnnealingLR), which lets the first
     steps cross the large blur of a metre-scale track error and the last ones
     settle.  Each step is replayed from a captured CUDA graph (graph=False:
     eager); entropies and parameters stay on the device and the steps are
-    timed with CUDA events, so the host never waits inside the loop."""
+    timed with CUDA events, so the host never waits inside the loop.
+
+    Checkpoints: the result's `state` holds the last iterate and Adam's
+    moments; `resume=state` continues from it (its learning rate and
+    schedule position), so a run of n steps split into parts that save and
+    resume their state reaches the same coefficients as the whole run.  The
+    cosine schedule spans `total_iters` steps (default: this call's steps,
+    or the resumed run's total)."""
     dev = motion.base.device
-    start = theta0.clone() if theta0 is not None else torch.zeros((3, 4), dtype=torch.float64, device=dev)
+    done = 0
+    if resume is not None:
+        lr = resume.lr
+        done = resume.iters_done
+        total = resume.total_iters if total_iters is None else int(total_iters)
+        start = torch.as_tensor(resume.theta, dtype=torch.float64, device=dev)
+    else:
+        total = iters if total_iters is None else int(total_iters)
+        start = theta0.clone() if theta0 is not None else torch.zeros((3, 4), dtype=torch.float64, device=dev)
     theta = start.clone().requires_grad_(True)
     lr_t = torch.tensor(lr, dtype=torch.float64, device=dev)
     opt = torch.optim.Adam([theta], lr=lr_t, capturable=True)
+    if resume is not None:
+        st = opt.state[theta]
+        # Adam's own lazy state: a scalar step tensor of the default scalar
+        # type on the device (capturable), moments of the parameter's type
+        step_dtype = torch.float64 if torch.get_default_dtype() == torch.float64 else torch.float32
+        st["step"] = torch.tensor(resume.step, dtype=step_dtype, device=dev)
+        st["exp_avg"] = torch.as_tensor(resume.exp_avg, dtype=torch.float64, device=dev).clone()
+        st["exp_avg_sq"] = torch.as_tensor(resume.exp_avg_sq, dtype=torch.float64, device=dev).clone()
     eta_min = lr / 100.0
 
     def lr_at(it):
-        return eta_min + 0.5 * (lr - eta_min) * (1.0 + math.cos(math.pi * it / iters)) if coarse_to_fine else lr
+        k = done + it
+        return eta_min + 0.5 * (lr - eta_min) * (1.0 + math.cos(math.pi * k / total)) if coarse_to_fine else lr
 
     e_out = torch.zeros((), dtype=torch.float64, device=dev)
     theta_pre = torch.zeros_like(start)
@@ -228,9 +282,14 @@ def gradient_autofocus(plan: Plan, motion: CubicMotion, slant_range, start_freq,
     seconds, events = _descend(step, iters, lr_at, lr_t, record, graph)
     e_host = ents.cpu().tolist()
     best = min(range(iters), key=lambda i: e_host[i])
-    hist = [{"iter": it, "entropy": e_host[it], "t": events[0].elapsed_time(events[it + 1]) * 1e-3}
+    hist = [{"iter": done + it, "entropy": e_host[it], "t": events[0].elapsed_time(events[it + 1]) * 1e-3}
             for it in range(iters) if (log_every and (it % log_every == 0 or it == iters - 1)) or not log_every]
-    return AutofocusResult(theta=thetas[best].clone(), history=hist, seconds=seconds, images_formed=iters)
+    ost = opt.state[theta]
+    state = AutofocusState(theta=theta.detach().cpu().numpy().copy(), exp_avg=ost["exp_avg"].cpu().numpy().copy(),
+                           exp_avg_sq=ost["exp_avg_sq"].cpu().numpy().copy(), step=float(ost["step"]),
+                           iters_done=done + iters, total_iters=total, lr=lr)
+    return AutofocusResult(theta=thetas[best].clone(), history=hist, seconds=seconds, images_formed=iters,
+                           state=state)
 
 
 # The reference's quadratic search varies, per axis, the slope and the

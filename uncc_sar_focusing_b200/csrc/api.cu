@@ -632,6 +632,7 @@ const char *sarbp_status_string(int status) {
 }
 
 int sarbp_plan_create(const sarbp_plan_desc *desc, sarbp_plan **out) {
+    NvtxRange range("sarbp_plan_create");
     if (!out) return SARBP_ERR_NULL_POINTER;
     *out = nullptr;
     int st = validate_desc(desc);
@@ -806,6 +807,7 @@ int sarbp_test_drop_window_copy(sarbp_plan *plan, int pulse) {
 }
 
 int sarbp_plan_set_range_weights(sarbp_plan *plan, const double *weights) {
+    NvtxRange range("sarbp_plan_set_range_weights");
     if (!plan) return SARBP_ERR_NULL_POINTER;
     if (weights)
         for (int k = 0; k < 2 * plan->K; ++k)
@@ -824,6 +826,7 @@ int sarbp_plan_set_range_weights(sarbp_plan *plan, const double *weights) {
 }
 
 int sarbp_range_compress(sarbp_plan *plan, const void *phase_history, int num_pulses, int memory, void *stream) {
+    NvtxRange range("sarbp_range_compress");
     if (!plan) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
@@ -832,6 +835,7 @@ int sarbp_range_compress(sarbp_plan *plan, const void *phase_history, int num_pu
 }
 
 int sarbp_get_range_profiles(sarbp_plan *plan, void *out, int memory, void *stream) {
+    NvtxRange range("sarbp_get_range_profiles");
     if (!plan || !out) return SARBP_ERR_NULL_POINTER;
     if (memory != SARBP_MEMORY_HOST && memory != SARBP_MEMORY_DEVICE) return SARBP_ERR_INVALID_ARGUMENT;
     if (plan->np_ready < 1) return SARBP_ERR_INVALID_ARGUMENT;
@@ -852,6 +856,7 @@ int sarbp_get_range_profiles(sarbp_plan *plan, void *out, int memory, void *stre
 
 int sarbp_backproject(sarbp_plan *plan, const sarbp_geometry *geometry, void *image, int image_memory, int flags,
                       void *stream) {
+    NvtxRange range("sarbp_backproject");
     if (!plan) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
@@ -860,13 +865,19 @@ int sarbp_backproject(sarbp_plan *plan, const sarbp_geometry *geometry, void *im
 }
 
 int sarbp_focus(sarbp_plan *plan, const sarbp_aperture *ap, void *image, int image_memory, void *stream) {
+    NvtxRange range("sarbp_focus");
     if (!plan || !ap) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
     SARBP_TRY(drain_pipe(plan));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int st = range_compress_impl(plan, ap->phase_history, ap->geometry.num_pulses, ap->phase_history_memory, s);
-    if (st != SARBP_OK) return st;
+    {
+        NvtxRange rc("range compression");
+        const int st = range_compress_impl(plan, ap->phase_history, ap->geometry.num_pulses,
+                                           ap->phase_history_memory, s);
+        if (st != SARBP_OK) return st;
+    }
+    NvtxRange bp("backprojection");
     return backproject_impl(plan, &ap->geometry, image, image_memory, 0, s);
 }
 
@@ -883,6 +894,7 @@ int sarbp_focus_image(const sarbp_plan_desc *desc, const sarbp_aperture *ap, voi
 
 int sarbp_backproject_hypotheses(sarbp_plan *plan, const sarbp_geometry *geometry, int num_hypotheses, void *images,
                                  int image_memory, int flags, void *stream) {
+    NvtxRange range("sarbp_backproject_hypotheses");
     if (!plan) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
@@ -894,6 +906,7 @@ int sarbp_backproject_hypotheses(sarbp_plan *plan, const sarbp_geometry *geometr
 int sarbp_backproject_adjoint(sarbp_plan *plan, const sarbp_geometry *geometry, const void *grad_image,
                               int grad_memory, double *grad_ant, double *grad_r0, int out_memory, int flags,
                               void *stream) {
+    NvtxRange range("sarbp_backproject_adjoint");
     if (!plan) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
@@ -903,6 +916,7 @@ int sarbp_backproject_adjoint(sarbp_plan *plan, const sarbp_geometry *geometry, 
 }
 
 int sarbp_focus_submit(sarbp_plan *plan, const sarbp_aperture *aperture, void *image, unsigned long long *ticket) {
+    NvtxRange range("sarbp_focus_submit");
     if (!plan) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
@@ -910,6 +924,7 @@ int sarbp_focus_submit(sarbp_plan *plan, const sarbp_aperture *aperture, void *i
 }
 
 int sarbp_focus_wait(sarbp_plan *plan, unsigned long long ticket) {
+    NvtxRange range("sarbp_focus_wait");
     if (!plan) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
@@ -918,6 +933,7 @@ int sarbp_focus_wait(sarbp_plan *plan, unsigned long long ticket) {
 
 int sarbp_matched_filter(sarbp_plan *plan, const sarbp_aperture *aperture, void *image, int image_memory,
                          void *stream) {
+    NvtxRange range("sarbp_matched_filter");
     if (!plan) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);
@@ -926,6 +942,7 @@ int sarbp_matched_filter(sarbp_plan *plan, const sarbp_aperture *aperture, void 
 }
 
 int sarbp_plan_check(sarbp_plan *plan, void *stream) {
+    NvtxRange range("sarbp_plan_check");
     if (!plan) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(plan->device);
     SARBP_TRY_CUDA(guard.status);

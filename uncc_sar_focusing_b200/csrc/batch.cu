@@ -334,6 +334,7 @@ int wait_impl(sarbp_batch *b, double *image_ms) {
 extern "C" {
 
 int sarbp_batch_create(const sarbp_plan_desc *descs, int num_scenes, sarbp_batch **out) {
+    NvtxRange range("sarbp_batch_create");
     if (!out || !descs) return SARBP_ERR_NULL_POINTER;
     *out = nullptr;
     if (num_scenes < 1 || num_scenes > 65535) return SARBP_ERR_INVALID_ARGUMENT;
@@ -494,6 +495,7 @@ int sarbp_batch_destroy(sarbp_batch *b) {
 }
 
 int sarbp_batch_focus(sarbp_batch *b, const sarbp_aperture *aps, void *const *images, void *stream) {
+    NvtxRange range("sarbp_batch_focus");
     if (!b) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(b->device);
     SARBP_TRY_CUDA(guard.status);
@@ -501,6 +503,7 @@ int sarbp_batch_focus(sarbp_batch *b, const sarbp_aperture *aps, void *const *im
 }
 
 int sarbp_batch_wait(sarbp_batch *b, double *image_ms) {
+    NvtxRange range("sarbp_batch_wait");
     if (!b) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(b->device);
     SARBP_TRY_CUDA(guard.status);
@@ -509,6 +512,7 @@ int sarbp_batch_wait(sarbp_batch *b, double *image_ms) {
 
 int sarbp_batch_autotune(sarbp_batch *b, const sarbp_aperture *aps, void *const *images, void *stream,
                          double *best_ms) {
+    NvtxRange range("sarbp_batch_autotune");
     if (!b) return SARBP_ERR_NULL_POINTER;
     if (!aps || !images) return SARBP_ERR_NULL_POINTER;
     DeviceGuard guard(b->device);

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cuda_runtime.h>
 #include <cufft.h>
+#include <nvtx3/nvToolsExt.h>
 #include <vector>
 
 #include "bp_common.cuh"
@@ -41,6 +42,16 @@ inline cudaError_t device_malloc(void **p, size_t bytes) {
     }
     return cudaMalloc(p, bytes);
 }
+
+// NVTX range over an entry point's host work (enqueueing, copies, waits), so
+// that Nsight Systems timelines and ncu's --nvtx filters can name the calls;
+// without a tool attached a push/pop costs a few nanoseconds.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 inline int from_cufft(cufftResult r) {
     if (r == CUFFT_SUCCESS) return SARBP_OK;

@@ -92,6 +92,7 @@ void axis(int n, double c, double w, double *lo, double *step) {
 extern "C" SARBP_API int sarbp_backproject_noalloc(const sarbp_plan_desc *desc, const void *range_profiles,
                                                    const sarbp_geometry *geo, void *image, int flags,
                                                    void *stream) {
+    host::NvtxRange range("sarbp_backproject_noalloc");
     if (!desc || !range_profiles || !geo || !image || !geo->ant_x || !geo->ant_y || !geo->ant_z ||
         !geo->slant_range || !geo->start_freq)
         return SARBP_ERR_NULL_POINTER;
