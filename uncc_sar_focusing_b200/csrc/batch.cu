@@ -51,6 +51,12 @@ struct sarbp_batch {
     BatchScene *h_table = nullptr, *d_table = nullptr;  // h_table page-locked
     void *d_partial = nullptr;
     size_t partial_bytes = 0;
+    // pre-pass geometry records of every scene, [scene][tile][pulse] at the
+    // current tile shape (null: the producers compute them)
+    void *d_geotab = nullptr;
+    size_t geotab_bytes = 0;
+    bool records_now = false;    // this call's table slots carry record rows
+    long long max_records = 0;   // the largest scene's tiles x pulses in this call
     unsigned long long *d_times = nullptr, *h_times = nullptr;  // [n] completion, [n] start; h page-locked
     unsigned *d_err = nullptr, *h_err = nullptr;
     long long units = 0, tiles = 0;
@@ -103,6 +109,7 @@ void release(sarbp_batch *b) {
     for (void *t : b->rc_tables) cudaFree(t);
     cudaFree(b->d_table);
     cudaFree(b->d_partial);
+    cudaFree(b->d_geotab);
     cudaFree(b->d_times);
     cudaFree(b->d_err);
     if (b->h_table) cudaFreeHost(b->h_table);
@@ -138,6 +145,24 @@ bool configure(sarbp_batch *b, const TileConfig &tc) {
         b->partial_bytes = 0;
         if (balloc(b, &b->d_partial, need) != SARBP_OK) return false;
         b->partial_bytes = need;
+    }
+    // room for every scene's records at this tile shape (environment
+    // SARBP_PREGEO=0, or no room: the producers compute the records)
+    const char *pregeo_env = std::getenv("SARBP_PREGEO");
+    if (!(pregeo_env && std::strcmp(pregeo_env, "0") == 0)) {
+        size_t recs = 0;
+        for (int i = 0; i < b->n; ++i) {
+            const sarbp_grid &g = b->desc[i].grid;
+            recs += static_cast<size_t>((g.ny + 63) / 64) * ((g.nx + 8 * tc.mx - 1) / (8 * tc.mx)) * g.nz *
+                    static_cast<size_t>(b->desc[i].num_pulses);
+        }
+        const size_t need = recs * sizeof(PulseGeo);
+        if (need > b->geotab_bytes) {
+            cudaFree(b->d_geotab);
+            b->d_geotab = nullptr;
+            b->geotab_bytes = 0;
+            if (balloc(b, &b->d_geotab, need) == SARBP_OK) b->geotab_bytes = need;
+        }
     }
     b->tile = tc;
     b->smem = smem;
@@ -240,6 +265,26 @@ int fill_table(sarbp_batch *b, const sarbp_aperture *aps, void *const *images) {
     }
     b->units = units;
     b->tiles = tiles;
+    // record rows of every scene at this call's pulse counts, [tile][pulse]
+    // per scene, back to back; all scenes or none
+    long long off = 0, biggest = 0;
+    for (int i = 0; i < b->n; ++i) {
+        const BpLaunch &L = b->h_table[i].L;
+        const long long r = tile::tile_grid(L, 8 * b->tile.mx, 1).tiles * L.np;
+        off += r;
+        biggest = r > biggest ? r : biggest;
+    }
+    b->records_now = b->d_geotab && static_cast<size_t>(off) * sizeof(PulseGeo) <= b->geotab_bytes &&
+                     biggest < 0x7fffffffLL;
+    b->max_records = biggest;
+    off = 0;
+    for (int i = 0; i < b->n; ++i) {
+        BpLaunch &L = b->h_table[i].L;
+        const long long r = tile::tile_grid(L, 8 * b->tile.mx, 1).tiles * L.np;
+        L.geo_tab = b->records_now ? static_cast<void *>(static_cast<PulseGeo *>(b->d_geotab) + off) : nullptr;
+        L.geo_tab_records = b->records_now ? r : 0;
+        off += r;
+    }
     return SARBP_OK;
 }
 
@@ -254,6 +299,8 @@ int enqueue(sarbp_batch *b, cudaStream_t s) {
     SARBP_TRY_CUDA(cudaMemsetAsync(b->d_times, 0, (n + 1) * sizeof(unsigned long long), s));
     stamp_kernel<<<1, 1, 0, s>>>(b->d_times + n);
     SARBP_TRY_CUDA(cudaGetLastError());
+    if (b->records_now)
+        SARBP_TRY_CUDA(launch_geo_records_batch(b->d_table, n, b->tile.mx, b->max_records, s));
     SARBP_TRY_CUDA(launch_rc_prep_batch(b->d_table, n, s));
     for (int i = 0; i < n; ++i) {
         if (b->rctab[i]) {
@@ -269,7 +316,8 @@ int enqueue(sarbp_batch *b, cudaStream_t s) {
     }
     SARBP_TRY_CUDA(launch_rc_pairs_batch(b->d_table, n, s));
     SARBP_TRY_CUDA(launch_bp_mixed_batch(b->d_table, n, b->units, b->tiles, b->tile, b->smem, b->resident,
-                                         b->d_partial, b->d_times, s, b->max_wsize, per_tile_now(b)));
+                                         b->d_partial, b->d_times, s, b->max_wsize, per_tile_now(b),
+                                         b->records_now ? b->d_geotab : nullptr));
     SARBP_TRY_CUDA(cudaMemcpyAsync(b->h_times, b->d_times, (n + 1) * sizeof(unsigned long long),
                                    cudaMemcpyDeviceToHost, s));
     SARBP_TRY_CUDA(cudaMemcpyAsync(b->h_err, b->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));

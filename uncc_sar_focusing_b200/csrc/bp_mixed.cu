@@ -376,16 +376,29 @@ __global__ void __launch_bounds__(kThreads, MINB)
 
     // records, base tables and windows of the producer cursor's unit into
     // buffer s
-    // Pre-pass records (single-scene launches): the records of the stage
-    // after the producer's are copied asynchronously into the staging ring
-    // (two stages of PB records after the stage buffers' windows) while the
-    // current stage accumulates, so their global-memory latency does not
-    // stall the producing warps.
-    const bool pregeo = !BATCH && L0.geo_tab != nullptr;
+    // Pre-pass records (single-scene launches: L0.geo_tab; batches: each
+    // scene's L.geo_tab, L0.geo_tab non-null when every scene has them): the
+    // records of the stage after the producer's are copied asynchronously
+    // into the staging ring (two stages of PB records after the stage
+    // buffers' windows) while the current stage accumulates, so their
+    // global-memory latency does not stall the producing warps.
+    const bool pregeo = L0.geo_tab != nullptr;
     PulseGeo *stg = reinterpret_cast<PulseGeo *>(smem + smem_bytes_of(PB, L0.wsize) - 2 * PB * sizeof(PulseGeo));
     // stage after the producer cursor's unit (last: the CTA has no more)
     auto prefetch_next = [&](int slot, bool last) {
         if (last) return;
+        if constexpr (BATCH) {
+            // the next unit may be the next scene's
+            SceneCursor<TX, PB, BATCH> nx = pc;
+            nx.advance(scenes, nscenes, rot_later);
+            const BpLaunch &L = *nx.L;
+            const long long t =
+                ((static_cast<long long>(nx.u.hyp) * L.nz + nx.u.iz) * nx.g.tiles_x + nx.u.tx) * nx.g.tiles_y +
+                nx.u.ty;
+            prefetch_records<PB>(L, static_cast<const PulseGeo *>(L.geo_tab) + t * L.np, nx.stage(),
+                                 stg + slot * PB, warp, lane);
+            return;
+        }
         const BpLaunch &L = *pc.L;
         long long t =
             ((static_cast<long long>(pc.u.hyp) * L.nz + pc.u.iz) * pc.g.tiles_x + pc.u.tx) * pc.g.tiles_y + pc.u.ty;
@@ -610,37 +623,52 @@ __global__ void __launch_bounds__(kThreads)
 // lanes of each 16-byte store on the same four banks).  Indexes are 32-bit:
 // the launch checks n < 2^31.
 template <int MX>
-__global__ void __launch_bounds__(256) bp_geo_records_kernel(const __grid_constant__ BpLaunch L, int n) {
+__device__ __forceinline__ void geo_records_chunk(const BpLaunch &L, unsigned n, unsigned i0, float4 *words) {
     constexpr int TX = 8 * MX;
     constexpr int kWords = sizeof(PulseGeo) / sizeof(float4);
     constexpr int kStride = 257;
-    __shared__ float4 words[kWords * kStride];
     const TileGrid tg = tile_grid(L, TX, 1);
     const unsigned np = static_cast<unsigned>(L.np), ty_n = static_cast<unsigned>(tg.tiles_y),
                    tx_n = static_cast<unsigned>(tg.tiles_x), nz = static_cast<unsigned>(L.nz);
-    float4 *out = static_cast<float4 *>(L.geo_tab);
-    for (unsigned i0 = blockIdx.x * 256u; i0 < static_cast<unsigned>(n); i0 += gridDim.x * 256u) {
-        const unsigned i = i0 + threadIdx.x;
-        if (i < static_cast<unsigned>(n)) {
-            const unsigned t = i / np, p = i - t * np;
-            const unsigned r = t / ty_n, ty = t - r * ty_n;
-            const unsigned zz = r / tx_n, tx = r - zz * tx_n;
-            const unsigned hyp = zz / nz, iz = zz - hyp * nz;
-            const double cx = L.left + static_cast<double>(static_cast<int>(tx) * TX + TX / 2) * L.dx;
-            const double cy = L.bottom + static_cast<double>(static_cast<int>(ty) * kTY + kTY / 2) * L.dy;
-            const double cz = L.zlow + static_cast<double>(iz) * L.dz;
-            const PulseGeo g = make_geo(L, static_cast<int>(p), static_cast<long long>(hyp) * L.np, cx, cy, cz, TX / 2);
-            const float4 *gw = reinterpret_cast<const float4 *>(&g);
+    const unsigned i = i0 + threadIdx.x;
+    if (i < n) {
+        const unsigned t = i / np, p = i - t * np;
+        const unsigned r = t / ty_n, ty = t - r * ty_n;
+        const unsigned zz = r / tx_n, tx = r - zz * tx_n;
+        const unsigned hyp = zz / nz, iz = zz - hyp * nz;
+        const double cx = L.left + static_cast<double>(static_cast<int>(tx) * TX + TX / 2) * L.dx;
+        const double cy = L.bottom + static_cast<double>(static_cast<int>(ty) * kTY + kTY / 2) * L.dy;
+        const double cz = L.zlow + static_cast<double>(iz) * L.dz;
+        const PulseGeo g = make_geo(L, static_cast<int>(p), static_cast<long long>(hyp) * L.np, cx, cy, cz, TX / 2);
+        const float4 *gw = reinterpret_cast<const float4 *>(&g);
 #pragma unroll
-            for (int k = 0; k < kWords; ++k) words[k * kStride + threadIdx.x] = gw[k];
-        }
-        __syncthreads();
-        const unsigned left = static_cast<unsigned>(n) - i0;
-        const int nw = static_cast<int>((left < 256u ? left : 256u) * kWords);
-        for (int w = threadIdx.x; w < nw; w += 256)
-            out[static_cast<long long>(i0) * kWords + w] = words[(w % kWords) * kStride + w / kWords];
-        __syncthreads();
+        for (int k = 0; k < kWords; ++k) words[k * kStride + threadIdx.x] = gw[k];
     }
+    __syncthreads();
+    float4 *out = static_cast<float4 *>(L.geo_tab);
+    const unsigned left = n - i0;
+    const int nw = static_cast<int>((left < 256u ? left : 256u) * kWords);
+    for (int w = threadIdx.x; w < nw; w += 256)
+        out[static_cast<long long>(i0) * kWords + w] = words[(w % kWords) * kStride + w / kWords];
+    __syncthreads();
+}
+
+template <int MX>
+__global__ void __launch_bounds__(256) bp_geo_records_kernel(const __grid_constant__ BpLaunch L, int n) {
+    __shared__ float4 words[(sizeof(PulseGeo) / sizeof(float4)) * 257];
+    for (unsigned i0 = blockIdx.x * 256u; i0 < static_cast<unsigned>(n); i0 += gridDim.x * 256u)
+        geo_records_chunk<MX>(L, static_cast<unsigned>(n), i0, words);
+}
+
+// The same for every scene of a batch (blockIdx.y = scene), into each
+// scene's record rows (BatchScene::L.geo_tab).
+template <int MX>
+__global__ void __launch_bounds__(256) bp_geo_records_batch_kernel(const BatchScene *__restrict__ scenes) {
+    __shared__ float4 words[(sizeof(PulseGeo) / sizeof(float4)) * 257];
+    const BpLaunch &L = scenes[blockIdx.y].L;
+    if (!L.geo_tab) return;
+    const unsigned n = static_cast<unsigned>(tile_grid(L, 8 * MX, 1).tiles) * static_cast<unsigned>(L.np);
+    for (unsigned i0 = blockIdx.x * 256u; i0 < n; i0 += gridDim.x * 256u) geo_records_chunk<MX>(L, n, i0, words);
 }
 
 template <int MX>
@@ -666,6 +694,22 @@ cudaError_t launch_geo_records(const BpLaunch &L, int mx, bool *ran, cudaStream_
         case 1: return launch_records_mx<1>(L, ran, s);
         default: *ran = false; return cudaSuccess;
     }
+}
+
+cudaError_t launch_geo_records_batch(const BatchScene *scenes, int nscenes, int mx, long long max_records,
+                                     cudaStream_t s) {
+    if (nscenes < 1 || nscenes > 65535 || max_records < 1 || max_records >= 0x7fffffffLL)
+        return cudaErrorInvalidValue;
+    const long long bx = (max_records + 255) / 256;
+    const dim3 grid(static_cast<unsigned>(bx < 1024 ? bx : 1024), static_cast<unsigned>(nscenes));
+    switch (mx) {
+        case 8: bp_geo_records_batch_kernel<8><<<grid, 256, 0, s>>>(scenes); break;
+        case 4: bp_geo_records_batch_kernel<4><<<grid, 256, 0, s>>>(scenes); break;
+        case 2: bp_geo_records_batch_kernel<2><<<grid, 256, 0, s>>>(scenes); break;
+        case 1: bp_geo_records_batch_kernel<1><<<grid, 256, 0, s>>>(scenes); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 namespace {
@@ -802,10 +846,12 @@ const int bp_batch_tile_count = static_cast<int>(sizeof(bp_batch_tiles) / sizeof
 
 cudaError_t launch_bp_mixed_batch(const BatchScene *scenes, int nscenes, long long units, long long tiles,
                                   const TileConfig &tc, size_t smem, int resident, void *partial,
-                                  unsigned long long *done, cudaStream_t s, int max_wsize, bool per_tile) {
+                                  unsigned long long *done, cudaStream_t s, int max_wsize, bool per_tile,
+                                  void *records) {
     BpLaunch L0{};
     L0.wsize = max_wsize;
     L0.sk_partial = partial;
+    L0.geo_tab = records;  // non-null: every scene's table slot has its record rows
 #define SARBP_BATCH_CASE(MX_, PB_) \
     if (tc.mx == MX_ && tc.pb == PB_)  \
         return launch_batch_mx_pb<MX_, PB_>(scenes, nscenes, units, tiles, smem, resident, L0, done, per_tile, s);

@@ -89,6 +89,11 @@ cudaError_t launch_bp_mixed(const BpLaunch &L, const TileConfig &tc, bool checke
 // L.geo_tab is null or holds fewer records than the launch has; the kernels
 // then compute the records themselves.
 cudaError_t launch_geo_records(const BpLaunch &L, int mx, bool *ran, cudaStream_t s);
+// The same for every scene of a batch whose table slot has record rows
+// (L.geo_tab non-null), tiles of (8 mx) x 64 pixels; max_records: the
+// largest scene's tiles x pulses.
+cudaError_t launch_geo_records_batch(const BatchScene *scenes, int nscenes, int mx, long long max_records,
+                                     cudaStream_t s);
 cudaError_t launch_bp_fp64(const BpLaunch &L, const TileConfig &tc, size_t smem, cudaStream_t s);
 size_t bp_mixed_smem_bytes(const TileConfig &tc, int wsize);
 // Adjoint (bp_adjoint.cu): per-(tile, pulse) gradient partials, then a sum
@@ -111,11 +116,14 @@ int bp_mixed_resident(const TileConfig &tc, size_t smem);
 // image (%globaltimer ns) goes to done[scene] (atomic max) when done != null.
 // max_wsize: the largest scene window (entries), the stage buffers' stride.
 // per_tile: one CTA per tile in scene order instead of the even split (no
-// partial sums; scenes complete one after another).
+// partial sums; scenes complete one after another).  records: non-null when
+// every scene's slot carries pre-pass record rows (launch_geo_records_batch
+// filled them), else the producers compute the records.
 // Instantiated for the tile shapes in bp_batch_tiles.
 cudaError_t launch_bp_mixed_batch(const BatchScene *scenes, int nscenes, long long units, long long tiles,
                                   const TileConfig &tc, size_t smem, int resident, void *partial,
-                                  unsigned long long *done, cudaStream_t s, int max_wsize, bool per_tile);
+                                  unsigned long long *done, cudaStream_t s, int max_wsize, bool per_tile,
+                                  void *records);
 int bp_mixed_batch_resident(const TileConfig &tc, size_t smem);
 extern const TileConfig bp_batch_tiles[];
 extern const int bp_batch_tile_count;
