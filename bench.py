@@ -348,8 +348,14 @@ def autofocus_section(dev, grid_seconds: float):
         ent = lambda x, y, z, r=r0: float(A.image_entropy(plan.backproject(x, y, z, r, f0)))  # noqa: E731
         e_measured = ent(ax, ay, az)
         e_true = ent(*(d(getattr(sc, a) + sc.true_error[i]) for i, a in enumerate(("ant_x", "ant_y", "ant_z"))))
-        AF.focus_motion_error(plan, ax, ay, az, r0, f0, cubic_iters=5, los_iters=5, pga_iters=1)  # warm-up
-        grad = AF.focus_motion_error(plan, ax, ay, az, r0, f0)
+        # warm-up past the descent's graph capture (its first 10 steps run eagerly)
+        AF.focus_motion_error(plan, ax, ay, az, r0, f0, cubic_iters=15, los_iters=15, pga_iters=1)
+        # three runs: the pipeline is deterministic (same entropies each run),
+        # its wall time is not (a host stall early in a run delays the steps
+        # that reach the target); the run of median total time is reported
+        runs = [AF.focus_motion_error(plan, ax, ay, az, r0, f0) for _ in range(3)]
+        runs.sort(key=lambda r: r["seconds"])
+        grad = runs[1]
         motion = AF.CubicMotion(ax, ay, az)
         searches = {}
         for cost in ("reference_dft", "entropy"):
@@ -363,14 +369,16 @@ def autofocus_section(dev, grid_seconds: float):
     def search_entry(cost):
         g, metrics = searches[cost]
         e = metrics["shannon_entropy"]
-        t = AF.time_to_entropy(grad["timeline"], e)
+        reach = [AF.time_to_entropy(r["timeline"], e) for r in runs]
+        t = None if any(x is None for x in reach) else sorted(reach)[1]  # median of the three runs
         return {"cost": cost, "entropy": e, "seconds": g.seconds, "images": g.images_formed,
                 "levels_done": len(g.history), "bounded_to_s": grid_seconds, "final_image": metrics,
                 "searched": "slope and quadratic term of each axis (the reference's quadratic search without "
                             "its velocity scale), 5 points each, box halved per level; the 12 cubic coefficients "
                             "at 5 points would be 5^12 images per level",
                 "sec_to_focus": {"target_entropy": e, "gradient_s": t, "grid_search_s": g.seconds,
-                                 "speedup": (g.seconds / t) if t else None}}
+                                 "speedup": (g.seconds / t) if t else None,
+                                 "gradient_s_runs": reach}}
     return {
         "workload": "autofocus: 9.6 GHz / 600 MHz, 4 deg at 10 km, 30 deg el, 1024 pulses x 512 samples, 512^2 "
                     "image at 0.08 m, 5 targets, 20 dB SNR; track error per axis = seeded cubic (1.5 m peak) + "
@@ -378,6 +386,7 @@ def autofocus_section(dev, grid_seconds: float):
         "entropy_measured_track": e_measured, "entropy_true_track": e_true,
         "gradient": {"entropy_cubic": grad["entropy_cubic"], "entropy_line_of_sight": grad["entropy_los"],
                      "entropy_pga": grad["entropy_pga"], "seconds": grad["seconds"],
+                     "seconds_runs": [r["seconds"] for r in runs],
                      "final_image": metrics_grad,
                      "stages": "Adam on 12 cubic coefficients (300 it) -> Adam on 1024 per-pulse ranges "
                                "(200 it) -> PGA (PGA.m semantics, on the device); gradients from the adjoint "

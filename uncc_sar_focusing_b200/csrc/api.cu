@@ -130,6 +130,7 @@ void release(sarbp_plan *p) {
     cudaFree(p->d_hyp);
     cudaFree(p->d_sk);
     cudaFree(p->d_geotab);
+    cudaFree(p->d_hyprec);
     cudaFree(p->d_rctab);
     cudaFree(p->d_win);
     delete p;
@@ -325,6 +326,7 @@ int hypotheses_impl(sarbp_plan *p, const sarbp_geometry *geo, int nhyp, void *im
     const size_t need = (geo->memory == SARBP_MEMORY_HOST ? 5 * ngeo * sizeof(double) : 0) +
                         (image_memory == SARBP_MEMORY_HOST ? img_bytes : 0);
     if (need > p->hyp_bytes) {
+        p->bytes -= p->hyp_bytes;
         cudaFree(p->d_hyp);
         p->d_hyp = nullptr;
         p->hyp_bytes = 0;
@@ -352,6 +354,33 @@ int hypotheses_impl(sarbp_plan *p, const sarbp_geometry *geo, int nhyp, void *im
     }
     BpLaunch L = launch_params(p, dg[0], dg[1], dg[2], dg[3], dg[4], np, dimg, flags);
     L.nhyp = nhyp;
+    // geometry records of every (hypothesis, tile, pulse) from the pre-pass
+    // in the plan's hypothesis records buffer, grown on demand (not while the
+    // stream is being captured; a failed allocation leaves the producers
+    // computing the records); plans without records (SARBP_PREGEO=0) skip it
+    L.geo_tab = nullptr;
+    L.geo_tab_records = 0;
+    if (p->d_geotab) {
+        const long long recs = static_cast<long long>(nhyp) * ((g.ny + 63) / 64) *
+                               ((g.nx + 8 * p->tile.mx - 1) / (8 * p->tile.mx)) * g.nz * np;
+        const size_t bytes = static_cast<size_t>(recs) * sizeof(PulseGeo);
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+            cudaGetLastError();
+            cap = cudaStreamCaptureStatusActive;
+        }
+        if (bytes > p->hyprec_bytes && cap == cudaStreamCaptureStatusNone) {
+            p->bytes -= p->hyprec_bytes;
+            cudaFree(p->d_hyprec);
+            p->d_hyprec = nullptr;
+            p->hyprec_bytes = 0;
+            if (alloc(p, &p->d_hyprec, bytes) == SARBP_OK) p->hyprec_bytes = bytes;
+        }
+        if (bytes <= p->hyprec_bytes) {
+            L.geo_tab = p->d_hyprec;
+            L.geo_tab_records = recs;
+        }
+    }
     SARBP_TRY_CUDA(launch_bp_mixed(L, p->tile, false, p->smem, s));
     if (image_memory == SARBP_MEMORY_HOST) {
         SARBP_TRY_CUDA(cudaMemcpyAsync(images, dimg, img_bytes, cudaMemcpyDeviceToHost, s));
@@ -396,6 +425,7 @@ int adjoint_impl(sarbp_plan *p, const sarbp_geometry *geo, const void *grad, int
     const long long ntiles = bp_tile_count(L, tc);
     const size_t need = static_cast<size_t>(ntiles) * p->np_cap * 16;
     if (p->partials_bytes < need) {
+        p->bytes -= p->partials_bytes;
         cudaFree(p->d_partials);
         p->d_partials = nullptr;
         p->partials_bytes = 0;

@@ -187,6 +187,8 @@ struct sarbp_plan {
     int rc_grid;      // its CTAs
     void *d_geotab;   // pre-pass geometry records (BpLaunch::geo_tab), tiles x np_cap PulseGeo
     long long geotab_records;
+    void *d_hyprec;   // pre-pass records of hypothesis launches (grown on first use)
+    size_t hyprec_bytes;
     void *d_sk;       // partial sums of tiles split over CTAs (BpLaunch::sk_partial)
     size_t sk_bytes;
     int sk_resident;  // resident CTAs of the plan's forward kernel
