@@ -124,6 +124,34 @@ def test_gradient_autofocus_resumes_from_a_saved_state(torch_cuda, tmp_path):
                        rtol=1e-12, atol=0)
 
 
+def test_gradient_autofocus_stops_on_a_plateau(torch_cuda):
+    """With a plateau tolerance the descent ends at a check once the best
+    entropy gained less than the tolerance over the last check_every steps;
+    the steps it ran are the whole run's first steps."""
+    torch = torch_cuda
+    from uncc_sar_focusing_b200 import autofocus as AF
+    from uncc_sar_focusing_b200 import focusing
+
+    sc = S.motion_error_scene(K=128, Np=256, n=128, spacing=0.16, peak=0.3, walk_sigma=5e-4, seed=12,
+                              device="cuda")
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    ax, ay, az, r0, f0 = (dev(v) for v in (sc.ant_x, sc.ant_y, sc.ant_z, sc.slant_range, sc.start_freq))
+    with focusing.Plan.for_scene(sc, "mixed") as plan:
+        plan.range_compress(dev(sc.phase_history))
+        motion = AF.CubicMotion(ax, ay, az)
+        full = AF.gradient_autofocus(plan, motion, r0, f0, iters=200, graph=False)
+        early = AF.gradient_autofocus(plan, motion, r0, f0, iters=200, graph=False, plateau=1e-2, check_every=20)
+    n = early.images_formed
+    assert n % 20 == 0 and 40 <= n < 200  # the first check that can stop is after 40 steps
+    e_full = np.array([h["entropy"] for h in full.history])
+    e_early = np.array([h["entropy"] for h in early.history])
+    assert len(e_early) == n
+    assert np.allclose(e_early, e_full[:n], rtol=1e-12, atol=0)
+    best = np.minimum.accumulate(e_full)
+    assert best[n - 21] - best[n - 1] < 1e-2  # the check that stopped it
+    assert all(best[k - 21] - best[k - 1] >= 1e-2 for k in range(40, n, 20))  # the earlier checks did not
+
+
 def test_reference_costs_on_the_gpu_match_the_transcriptions(torch_cuda):
     """The reference's two grid-search costs, batched on the device, against
     direct transcriptions of the reference's loops (dft2DCalculation,
