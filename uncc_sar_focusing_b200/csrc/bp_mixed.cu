@@ -413,8 +413,9 @@ __global__ void __launch_bounds__(kThreads, MINB)
         prefetch_records<PB>(L, static_cast<const PulseGeo *>(L.geo_tab) + t * L.np, st, stg + slot * PB, warp, lane);
     };
     auto produce = [&](int s, const PulseGeo *staged) {
-        // every lane of the warp enters: produce_slots gives lane 0 the record
-        // and the copy and uses the whole warp (shuffles) for the base tables
+        // every lane of the warp enters: the base tables take the whole warp
+        // (the records come from the staging slot, or lane 0 computes them
+        // and shuffles their steps to the warp), lane 0 issues the copy
         const BpLaunch &L = *pc.L;
         const double cx = L.left + static_cast<double>(pc.u.tx * TX + TX / 2) * L.dx;
         const double cy = L.bottom + static_cast<double>(pc.u.ty * kTY + kTY / 2) * L.dy;
@@ -461,7 +462,8 @@ __global__ void __launch_bounds__(kThreads, MINB)
             if (pregeo) {
                 // stage i + 1's records were prefetched into staging slot
                 // (i + 1) & 1; stage i + 2's go to the other one, whose
-                // records stage i's producer read before the last barrier
+                // records this warp read when it produced stage i (a warp
+                // fills and reads only its own pulse slots of the ring)
                 produce(s ^ 1, stg + (s ^ 1) * PB);
                 prefetch_next(s, i + 2 >= n);
             } else {

@@ -214,10 +214,11 @@ constexpr int kBaseEntries = kWarps + 32 / 4;
 
 // Records (and base tables when base_s != nullptr) and window copies of
 // stage b into one buffer.  Warp w produces slots w, w + 8, ...: lane 0
-// computes the FP64 record, the warp's lanes fill the base tables from it,
-// then lane 0 issues the window's bulk copy (or a plain arrival), whose
-// release on the stage's mbarrier also publishes the tables (__syncwarp
-// orders the other lanes' stores before it).
+// computes the FP64 record (or lanes 0..7 move the prefetched pre-pass
+// record into place), the warp's lanes fill the base tables from it, then
+// lane 0 issues the window's bulk copy (or a plain arrival), whose release
+// on the stage's mbarrier also publishes the record and the tables
+// (__syncwarp orders the other lanes' stores before it).
 // Pre-pass records (BpLaunch::geo_tab) of pulse stage b of the tile whose
 // record row is `rec` into a staging slot of shared memory, asynchronously
 // (cp.async, 16 bytes by each of lanes 0..7 of warp q for slot q): issued a
