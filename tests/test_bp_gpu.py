@@ -171,19 +171,25 @@ def test_non_finite_geometry_is_reported(F):
         assert ei.value.status == F.N.SARBP_ERR_NOT_FINITE
 
 
-def test_large_config_sampled_pixels(F):
+def test_large_config_full_image(F):
     # the large configuration at full size: 1024 samples x 2048 pulses, 2000
-    # Rayleigh scatterers, 1024^2 over 100 m; checked on 3000 pixels
+    # Rayleigh scatterers, 1024^2 over 100 m; every pixel of the mixed and of
+    # the FP64 image against the FP64 CPU oracle (2.1e9 pixel-pulses on the
+    # host's cores: seconds on a 16-core host)
     import torch
 
     sc = S.large_scene(device="cuda")
     img = F.focus_scene(sc, "mixed")
-    rng = np.random.default_rng(0)
-    pix = np.sort(rng.choice(img.size, 3000, replace=False))
-    want = O.focus_fp64(sc, pixels=pix)
-    got = img.reshape(-1)[pix]
-    assert O.rel_l2(got, want) < MIXED_TOL
+    img64 = F.focus_scene(sc, "fp64")
+    want = O.focus_fp64(sc)
     assert np.isfinite(img).all()
+    err = O.rel_l2(img, want)
+    assert err < MIXED_TOL, err
+    # the mixed path's documented accuracy on this workload is ~2.2e-6
+    assert err < 1e-5, err
+    err64 = O.rel_l2(img64, want)
+    print(f"large configuration, full image vs FP64 oracle: mixed {err:.3e}, fp64 {err64:.3e}")
+    assert err64 < FP64_TOL, err64
     torch.cuda.empty_cache()
 
 
