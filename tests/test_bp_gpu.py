@@ -208,6 +208,27 @@ def test_volumetric_config_per_slice(F):
     assert O.rel_l2(got64, want) < FP64_TOL
 
 
+def test_volumetric_config_full_size_slices(F):
+    """The volumetric configuration at full size (8 passes x 1024 pulses x 512
+    samples, 256 x 256 x 64 voxels, Nfft 4096): four whole z-slices (bottom,
+    two inner, top; 2.1e9 voxel-pulses) of the mixed volume against the FP64
+    CPU oracle, each within 1e-4."""
+    import torch
+
+    sc = S.volumetric_scene(device="cuda")
+    got = F.focus_scene(sc, "mixed")
+    assert got.shape == (64, 256, 256)
+    assert np.isfinite(got).all()
+    zs = (0, 21, 42, 63)
+    plane = 256 * 256
+    pix = np.concatenate([np.arange(z * plane, (z + 1) * plane) for z in zs])
+    want = O.focus_fp64(sc, pixels=pix).reshape(len(zs), 256, 256)
+    per_slice = [O.rel_l2(got[z], want[i]) for i, z in enumerate(zs)]
+    print("volumetric configuration, slices", zs, "vs FP64 oracle:", ["%.2e" % e for e in per_slice])
+    assert max(per_slice) < MIXED_TOL, per_slice
+    torch.cuda.empty_cache()
+
+
 @pytest.mark.parametrize("K,R", [(256, 8), (512, 8), (1024, 8), (512, 1), (256, 16), (1024, 2)])
 def test_fused_range_compression_matches_oracle(F, K, R, monkeypatch):
     """nfft = R K with K in {256, 512, 1024} takes the fused range-compression
