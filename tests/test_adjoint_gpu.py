@@ -64,6 +64,17 @@ def test_adjoint_partial_last_stage(torch_cuda):
     assert ea < GRAD_TOL and er < GRAD_TOL, (ea, er)
 
 
+def test_adjoint_large_config(torch_cuda):
+    """The large configuration at full size (1024 x 2048 pulses, 1024^2
+    image, Nfft 8192) with a random upstream gradient: every pulse's dL/d
+    antenna xyz and dL/dR0 against the FP64 gradient oracle."""
+    sc = S.large_scene(device="cuda")
+    ea, er = grads_vs_oracle(torch_cuda, sc, seed=4)
+    print(f"large configuration adjoint vs FP64 gradient oracle: antenna {ea:.2e}, R0 {er:.2e} of max")
+    assert ea < GRAD_TOL and er < GRAD_TOL, (ea, er)
+    torch_cuda.cuda.empty_cache()
+
+
 def test_adjoint_near_field(torch_cuda):
     sc = S.point_target_scene(K=64, Np=32, n=64, spacing=0.1, nfft=512, snr_db=None, seed=7, n_targets=3,
                               radius=60.0)
