@@ -1,4 +1,6 @@
 """Hypothesis batches and the gradient autofocus pipeline on the GPU."""
+import copy
+
 import numpy as np
 import pytest
 
@@ -39,6 +41,48 @@ def test_hypothesis_batch_equals_single_images(torch_cuda):
             torch.cuda.synchronize()
             assert torch.equal(batch[h], one)
             assert np.array_equal(host[h], one.cpu().numpy())
+
+
+def test_hypothesis_batch_full_size_against_oracle(torch_cuda):
+    """The autofocus configuration at full size (1024 pulses x 512 samples,
+    512^2 image): 8 track hypotheses in one launch, the first and the last
+    against the FP64 CPU oracle on every pixel, all 8 against single calls.
+    At this size a single image's tiles are split over the resident CTAs and
+    their pulse stages summed in a rotated order, so the two agree to
+    rounding, not bit for bit (the small-scene test above has one CTA per
+    tile in both and is bit-exact)."""
+    torch = torch_cuda
+    from oracle import oracle as O
+    from uncc_sar_focusing_b200 import focusing
+
+    sc = S.motion_error_scene(device="cuda")
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    H = 8
+    rng = np.random.default_rng(1)
+    ramp = np.linspace(-1.0, 1.0, sc.num_pulses)
+    tracks = [np.stack([sc.ant_x, sc.ant_y, sc.ant_z]) + rng.normal(0, 0.02, (3, 1)) * ramp for _ in range(H)]
+    with focusing.Plan.for_scene(sc, "mixed") as plan:
+        plan.range_compress(dev(sc.phase_history))
+        r0 = dev(np.tile(sc.slant_range, (H, 1)))
+        f0 = dev(np.tile(sc.start_freq, (H, 1)))
+        ax, ay, az = (dev(np.stack([t[i] for t in tracks])) for i in range(3))
+        batch = plan.backproject_hypotheses(ax, ay, az, r0, f0)
+        for h in range(H):
+            one = plan.backproject(ax[h].contiguous(), ay[h].contiguous(), az[h].contiguous(), r0[h].contiguous(),
+                                   f0[h].contiguous())
+            torch.cuda.synchronize()
+            d = float((batch[h] - one).abs().pow(2).sum().sqrt() / one.abs().pow(2).sum().sqrt())
+            assert d < 1e-6, (h, d)
+        plan.check()
+        got = batch.cpu().numpy()
+    errs = []
+    for h in (0, H - 1):
+        sh = copy.copy(sc)
+        sh.ant_x, sh.ant_y, sh.ant_z = (np.ascontiguousarray(v) for v in tracks[h])
+        errs.append(O.rel_l2(got[h].reshape(-1), O.focus_fp64(sh).reshape(-1)))
+    print("hypotheses 0 and 7 vs FP64 oracle:", ["%.2e" % e for e in errs])
+    assert max(errs) < 1e-4, errs
+    torch.cuda.empty_cache()
 
 
 def test_gradient_autofocus_pipeline_recovers_focus(torch_cuda):
