@@ -192,3 +192,23 @@ def test_fused_range_compression_scenes_in_a_batch(F):
         got = img.cpu().numpy()
         assert O.rel_l2(got, O.focus_fp64(sc)) < 1e-4
         assert O.rel_l2(got, single(F, sc, tile=tile)) < 1e-5
+
+
+def test_batch_at_the_batched_configurations_sizes(F):
+    """Scenes of the batched configuration's size range (512 samples, Nfft
+    4096, 0.1 m pixels; 128^2 x 256 pulses up to 1024^2 x 2048 pulses) in
+    one batch: every image against the FP64 CPU oracle (3.1e9 pixel-pulses
+    on the host's cores)."""
+    import torch
+
+    shapes = [(128, 256, 5), (384, 1024, 60), (700, 777, 200), (1024, 2048, 500), (200, 1500, 30)]
+    scenes = [S.point_target_scene(K=512, Np=npulse, n=n, spacing=0.1, n_targets=nt, nfft=4096, seed=200 + i,
+                                   extent=0.08 * n, device="cuda") for i, (n, npulse, nt) in enumerate(shapes)]
+    with F.Batch(scenes) as batch:
+        imgs = batch.new_images()
+        batch.focus([dev_args(sc) for sc in scenes], imgs)
+        batch.wait()
+    errs = [O.rel_l2(img.cpu().numpy(), O.focus_fp64(sc)) for sc, img in zip(scenes, imgs)]
+    print("batched-configuration sizes vs FP64 oracle:", ["%.2e" % e for e in errs])
+    assert max(errs) < 1e-4, errs
+    torch.cuda.empty_cache()
