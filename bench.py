@@ -238,7 +238,8 @@ def reference_gpu_rate(scene, img64=None, reps: int = 3):
         return {"unavailable": "oracle/_ref/libref_gpu.so not built (needs the reference sources at build time)"}
     try:
         img, fft_ms, bp_ms = O.reference_gpu_focus(scene, reps=reps)
-    except ValueError as e:
+    except (ValueError, RuntimeError) as e:
+        # e.g. no CUDA device on this host: the CPU line still stands
         return {"unavailable": str(e)}
     pp = scene.pixel_pulses
     out = {"value": pp / (bp_ms * 1e-3), "unit": UNIT, "bp_ms": bp_ms, "range_compress_ms": fft_ms,
