@@ -312,6 +312,23 @@ SARBP_API int sarbp_batch_set_schedule(sarbp_batch *batch, int per_tile);
 SARBP_API int sarbp_matched_filter(sarbp_plan *plan, const sarbp_aperture *aperture, void *image, int image_memory,
                                    void *stream);
 
+/* The autofocus loss on the device.  Shannon entropy of a complex64 image's
+ * normalised intensity, E = -sum p log p with p = |I|^2 / sum |I|^2, the
+ * objective the gradient autofocus descends (no counterpart in the
+ * reference, whose grid search scores images with a 2-D DFT cost,
+ * src/autofocus/gridSearchErrorFunctions_dft.cuh:112-203).  `image` is n
+ * complex64 values in device memory; `work` is device memory of
+ * sarbp_image_entropy_work_bytes() bytes that keeps the sums for the
+ * gradient call; `entropy` (device float, may be NULL) receives E.  Sums in
+ * FP64 in a fixed order: repeatable bit for bit.  Asynchronous on `stream`.
+ * The gradient call writes grad_image = g * dE/d(Re I) + j g * dE/d(Im I)
+ * for the upstream scalar g = *grad_entropy (device float; NULL: 1), from
+ * the `work` of the sarbp_image_entropy call on the same image. */
+SARBP_API size_t sarbp_image_entropy_work_bytes(void);
+SARBP_API int sarbp_image_entropy(const void *image, long long n, void *work, float *entropy, void *stream);
+SARBP_API int sarbp_image_entropy_grad(const void *image, long long n, const void *work, const float *grad_entropy,
+                                       void *grad_image, void *stream);
+
 /* One call, no plan kept: create, focus, destroy (host or device buffers). */
 SARBP_API int sarbp_focus_image(const sarbp_plan_desc *desc, const sarbp_aperture *aperture, void *image,
                       int image_memory);

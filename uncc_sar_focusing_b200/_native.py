@@ -43,7 +43,8 @@ EXPORTED = (
     "sarbp_backproject_adjoint", "sarbp_backproject_hypotheses", "sarbp_focus_submit", "sarbp_focus_wait", "sarbp_plan_get_info",
     "sarbp_batch_create", "sarbp_batch_destroy", "sarbp_batch_focus", "sarbp_batch_wait", "sarbp_batch_autotune",
     "sarbp_batch_get_info", "sarbp_batch_set_schedule", "sarbp_matched_filter", "sarbp_plan_set_range_weights",
-    "sarbp_test_fail_device_alloc", "sarbp_test_drop_window_copy",
+    "sarbp_test_fail_device_alloc", "sarbp_test_drop_window_copy", "sarbp_image_entropy_work_bytes",
+    "sarbp_image_entropy", "sarbp_image_entropy_grad",
 )
 
 
@@ -126,9 +127,13 @@ def lib():
         L.sarbp_plan_set_range_weights.argtypes = [vp, vp]
         L.sarbp_test_fail_device_alloc.argtypes = [i]
         L.sarbp_test_drop_window_copy.argtypes = [vp, i]
+        L.sarbp_image_entropy_work_bytes.argtypes = []
+        L.sarbp_image_entropy.argtypes = [vp, ctypes.c_longlong, vp, vp, vp]
+        L.sarbp_image_entropy_grad.argtypes = [vp, ctypes.c_longlong, vp, vp, vp, vp]
         for name in EXPORTED:
             if name != "sarbp_status_string":
                 getattr(L, name).restype = i
+        L.sarbp_image_entropy_work_bytes.restype = ctypes.c_size_t
         _LIB = L
     return _LIB
 

@@ -41,7 +41,8 @@ REFERENCE_INCLUDE = os.path.join(REFERENCE, "include") if REFERENCE else ""
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
                   "-Xptxas", "-v", "--expt-relaxed-constexpr", "-ccbin", "g++"]
-SOURCES = ["api.cu", "batch.cu", "range_compress.cu", "bp_mixed.cu", "bp_fp64.cu", "bp_adjoint.cu", "noalloc.cu", "mf.cu"]
+SOURCES = ["api.cu", "batch.cu", "range_compress.cu", "bp_mixed.cu", "bp_fp64.cu", "bp_adjoint.cu", "noalloc.cu", "mf.cu",
+           "entropy.cu"]
 HEADERS = ["bp_common.cuh", "bp_tile.cuh", "sarbp_internal.h", "host_common.h"]
 
 
